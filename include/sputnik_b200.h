@@ -1,0 +1,225 @@
+/*
+ * sputnik_b200.h -- handle-based C ABI of libsputnik_b200.so, the B200
+ * (sm_100a) implementation of the sputnik micro-RVE homogenization path.
+ *
+ * These entry points have no one-to-one counterpart in the reference: they
+ * replace the micro program's homogenization driver (micro/src/homogenize.c,
+ * micro/src/assembly.c, micro/src/init.c, micro/src/alloc.c) and its MPI
+ * request loop (micro/src/main.c:114-153, inc/comm.h:18-27) with library
+ * calls that keep matrices, solutions and work queues on the GPU.  Each
+ * declaration names the reference code it stands in for.
+ *
+ * Conventions (as in the reference): every function returns int, 0 on
+ * success, a small positive code on failure; the message of the last failure
+ * on the calling thread is in sp_last_error().  No function aborts, traps or
+ * falls back to the CPU: without a usable CUDA device the compute calls
+ * return SP_ERR_CUDA.
+ *
+ * 3D conventions: node (i,j,k) -> i + j*nx + k*nx*ny, dof = 3*node + d;
+ * hexa8 local node order of the reference's src/fem.c:324-362; Voigt order
+ * (xx, yy, zz, xy, yz, xz) with engineering shear strains.
+ */
+#ifndef SPUTNIK_B200_H
+#define SPUTNIK_B200_H
+
+#include <stddef.h>
+
+#include "ell.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SP_OK 0
+#define SP_ERR_ARG 1     /* bad argument or unsupported size */
+#define SP_ERR_NOMEM 2   /* host or device allocation failed */
+#define SP_ERR_RANGE 3   /* index outside the object */
+#define SP_ERR_CUDA 5    /* no usable device or a CUDA call failed */
+#define SP_ERR_NOCONV 6  /* a solve stopped at its iteration limit */
+#define SP_ERR_BUDGET 7  /* request exceeds the HBM admission budget */
+#define SP_ERR_TIMEOUT 8 /* a bounded device wait gave up */
+#define SP_ERR_STATE 9   /* call not valid in the object's state */
+#define SP_PENDING 10    /* sp_server_poll: result not ready yet */
+
+#define SP_ID_MATRIX 0 /* micro/inc/micro_struct.h:13 */
+#define SP_ID_FIBER 1  /* micro/inc/micro_struct.h:14 */
+
+#define SP_MAX_RHS 8
+#define SP_ELL_WIDTH 81 /* 3D ELL row width, micro/src/alloc.c:6 */
+
+const char *sp_last_error(void);
+int sp_version(void);
+/* Select the CUDA device used by this thread's later calls (default 0). */
+int sp_init(int device);
+/* Number of usable CUDA devices (0 without a driver or GPU; never fails). */
+int sp_device_count(void);
+
+/* ------------------------------------------------------------- ELL extras */
+
+/* src/ell.c:103-118 with the column cleared in every row (the reference
+ * stops at the first empty slot of any row).  Host operation. */
+int ell_set_zero_col_full(ell_matrix *m, int col, double diag_val);
+/* Frees what ell_init allocated (the reference has no free). */
+int ell_free(ell_matrix *m);
+
+/* A copy of an ell_matrix resident on the GPU (rows padded to 84 slots). */
+typedef struct sp_ell_dev_s sp_ell_dev;
+int sp_ell_upload(const ell_matrix *m, sp_ell_dev **out);
+int sp_ell_dev_free(sp_ell_dev *a);
+/* y = A x with device pointers on `stream` (cudaStream_t, NULL = library
+ * stream): one warp per row, 128-bit loads.  Result within rounding of the
+ * reference's ell_mvp (src/ell.c:127-141). */
+int sp_ell_dev_mvp(sp_ell_dev *a, const double *x_dev, double *y_dev, void *stream);
+/* Same with host vectors (copies in and out). */
+int sp_ell_dev_mvp_host(sp_ell_dev *a, const double *x, double *y);
+/* Jacobi-preconditioned CG in FP64 on host vectors: the ELL path of the
+ * reference's solve() (micro/src/homogenize.c:320-333) with PETSc's
+ * KSPCG + PCJACOBI algorithm; stops at ||b - A x|| <= rtol ||b||.  x holds
+ * the initial guess on entry. */
+int sp_ell_dev_pcg(sp_ell_dev *a, const double *b, double *x, double rtol, int max_its,
+                   int *its, double *relres);
+
+/* --------------------------------------------------------------------- RVE */
+
+/* One structured micro-RVE: mesh (src/mesh.c:762-867 extended to 3D),
+ * fiber_cilin micro-structure (micro/src/micro_struct.c:3-37) and two linear
+ * elastic materials (src/material.c:84-135). */
+typedef struct {
+  int n[3];       /* elements per axis (the reference's -struct_n minus 1) */
+  double len[3];  /* RVE edge lengths (the micro_struct size) */
+  int nx_fib, ny_fib;
+  double radius;  /* fiber radius, element in fiber if centroid distance <= radius */
+  double desv[2]; /* fiber offset from the centre */
+  double E[2];    /* Young's modulus: [SP_ID_MATRIX], [SP_ID_FIBER] */
+  double nu[2];   /* Poisson ratio:  [SP_ID_MATRIX], [SP_ID_FIBER] */
+} sp_rve_desc;
+
+typedef struct {
+  int status;    /* 0 converged, SP_ERR_NOCONV otherwise */
+  int outer_its; /* Newton / refinement steps (max over rhs) */
+  int inner_its; /* CG iterations summed over steps (max over rhs) */
+  int pad;
+  double relres; /* final ||r(u)||/||r(u0)|| of the FP64 residual (max over rhs) */
+} sp_solve_info;
+
+/* Host-side element classification (micro/src/micro_struct.c:98-129 applied
+ * as micro/src/micro_struct.c:176-185); fills etype[nelm]. */
+int sp_classify(const sp_rve_desc *d, unsigned char *etype);
+/* ELL pattern of an n[0] x n[1] x n[2] mesh in the reference's first-touch
+ * insertion order (src/ell.c:46-73 driven by micro/src/assembly.c:93-110):
+ * cols[ndof*81], -1 padded.  Host operation. */
+int sp_ell_pattern(const int *n, int *cols);
+
+typedef struct sp_rve_s sp_rve;
+/* Builds the mesh plan, classifies elements, uploads and assembles the FP64
+ * ELL Jacobian on the GPU (micro/src/assembly.c:84-137 with every boundary
+ * row and column cleared). */
+int sp_rve_create(const sp_rve_desc *d, sp_rve **out);
+int sp_rve_destroy(sp_rve *r);
+int sp_rve_sizes(const sp_rve *r, int *ndof, int *nelm, int *nfiber);
+/* Downloads the assembled matrix in the reference layout (81 slots a row). */
+int sp_rve_get_ell(sp_rve *r, int *cols, double *vals);
+/* Per-material element stiffness (24x24, row-major) computed on the GPU. */
+int sp_rve_get_ke(sp_rve *r, double *ke_matrix, double *ke_fiber);
+/* Plain FP64 homogenization of nrhs macro strains (strains[nrhs][6]), one
+ * RVE and one GPU kernel sequence at a time: micro/src/homogenize.c:175-225
+ * (set_disp_0, Newton, Jacobi-PCG solve, add_x_dx) and :344-368 (averages).
+ * Converged when ||r(u)|| <= rtol ||r(u0)||.  Outputs are host arrays
+ * [nrhs][6]; u_out (optional) is [nrhs][ndof]. */
+int sp_rve_homogenize(sp_rve *r, int nrhs, const double *strains, double rtol,
+                      double *strain_ave, double *stress_ave, double *u_out, sp_solve_info *info);
+/* 6x6 homogenized tangent C[i][j] = <sigma_i>(e_j) from six unit-strain load
+ * cases solved together as one 6-rhs CG. */
+int sp_rve_tangent(sp_rve *r, double rtol, double *C, sp_solve_info *info);
+
+/* ------------------------------------------------------------------ batch */
+
+#define SP_PREC_MIXED 0 /* FP32 ELL values + FP32 CG, FP64 residual refinement */
+#define SP_PREC_FP64 1  /* FP64 values and CG */
+
+typedef struct {
+  int nrhs;          /* load cases per RVE, 1..8 (default 6) */
+  int precision;     /* SP_PREC_MIXED (default) or SP_PREC_FP64 */
+  double rtol;       /* FP64 residual target per rhs (default 1e-8) */
+  double inner_rtol; /* FP32 CG reduction per refinement step (default 1e-5) */
+  int max_outer;     /* refinement steps (default 8) */
+  int max_inner;     /* CG iterations per step (default 4000) */
+  int threads;       /* threads per CTA (0: tuned) */
+  int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
+  int ctas_per_sm;   /* resident CTAs per SM (0: tuned) */
+  int pad;
+} sp_batch_opts;
+
+void sp_batch_opts_default(sp_batch_opts *o);
+
+typedef struct sp_batch_s sp_batch;
+/* nrve independent RVEs of any mix of sizes.  Classifies elements on the
+ * host, builds one mesh plan per distinct size, allocates every RVE's ELL
+ * values and the per-CTA work space on the GPU. */
+int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batch_opts *o, sp_batch **out);
+int sp_batch_destroy(sp_batch *b);
+/* Bytes of device memory held by the batch. */
+int sp_batch_device_bytes(const sp_batch *b, size_t *bytes);
+/* Queue the host->device copy of the step's inputs on `stream`:
+ * strains[nrve][nrhs][6] (NULL: unit strains e_0..e_{nrhs-1}) and
+ * materials[nrve][4] = (E_matrix, nu_matrix, E_fiber, nu_fiber) (NULL: from
+ * the descriptors).  Host arrays should be pinned for asynchronous copies. */
+int sp_batch_upload(sp_batch *b, const double *strains, const double *materials, void *stream);
+/* One persistent launch: every RVE is assembled (coloured scatter into its
+ * ELL), solved for all load cases to rtol and volume-averaged. */
+int sp_batch_launch(sp_batch *b, void *stream);
+/* Queue the device->host copy of the results: stress[nrve][nrhs][6],
+ * strain[nrve][nrhs][6] (either may be NULL), info[nrve] (may be NULL). */
+int sp_batch_download(sp_batch *b, double *stress, double *strain, sp_solve_info *info,
+                      void *stream);
+/* upload + launch + download + synchronize: the end-to-end call. */
+int sp_batch_homogenize(sp_batch *b, const double *strains, const double *materials,
+                        double *stress, double *strain, sp_solve_info *info, void *stream);
+/* Kernel launches made by the last sp_batch_launch (for accounting). */
+int sp_batch_last_launches(const sp_batch *b, int *launches);
+
+/* ---------------------------------------------------------------- serving */
+
+/* A device-resident request loop standing in for the micro process's MPI
+ * request loop (micro/src/main.c:114-153): requests carry a macro strain and
+ * a geometry id and return the volume-averaged stress and the 6x6 tangent
+ * (finite differences with delta 0.005, micro/src/homogenize.c:59-94), solved
+ * as 7 load cases warm-started from that geometry's previous solution. */
+typedef struct {
+  size_t hbm_budget;    /* admission budget in bytes (0: 150 GB) */
+  int max_inflight;     /* request slots solving at once (0: one per CTA) */
+  int queue_capacity;   /* request ring size (0: 65536) */
+  double rtol;          /* default 1e-8 */
+  double inner_rtol;    /* default 1e-5 */
+  int idle_spin_limit;  /* empty polls before the loop returns (0: default) */
+  int pad;
+} sp_server_opts;
+
+void sp_server_opts_default(sp_server_opts *o);
+
+typedef struct sp_server_s sp_server;
+/* Makes every geometry resident (assembled FP32 ELL, FP64 element
+ * operators, warm-start store) while the running total stays within the
+ * budget; returns SP_ERR_BUDGET, creating nothing, if it does not. */
+int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_server_opts *o,
+                     sp_server **out);
+int sp_server_destroy(sp_server *s);
+/* Bytes the server would need for these geometries (no allocation). */
+int sp_server_plan_bytes(int ngeom, const sp_rve_desc *descs, const sp_server_opts *o,
+                         size_t *bytes);
+/* Starts the device loop (a persistent kernel polling the request ring). */
+int sp_server_start(sp_server *s);
+/* Enqueue one request; returns its ticket (0, 1, 2, ...). */
+int sp_server_submit(sp_server *s, int geometry, const double *strain, long long *ticket);
+/* SP_OK and the results when the ticket is done, SP_PENDING otherwise.
+ * stress[6], tangent[36] (row-major C[i][j] = d sigma_i / d eps_j). */
+int sp_server_poll(sp_server *s, long long ticket, double *stress, double *tangent,
+                   sp_solve_info *info);
+/* Stops the device loop after the queued requests finish. */
+int sp_server_stop(sp_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,388 @@
+"""madmax_b200 -- Python view of libsputnik_b200.so, the B200 (sm_100a)
+implementation of sputnik's micro-RVE homogenization hot path.
+
+The product is the C ABI in include/*.h; this module binds it with ctypes for
+the tests, the benchmark and Python callers.  It has no compute of its own and
+no fallback: if the shared library is missing it raises at import, and without
+a CUDA device the compute calls raise SputnikError(SP_ERR_CUDA).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsputnik_b200.so")
+
+SP_OK, SP_ERR_ARG, SP_ERR_NOMEM, SP_ERR_RANGE = 0, 1, 2, 3
+SP_ERR_CUDA, SP_ERR_NOCONV, SP_ERR_BUDGET, SP_ERR_TIMEOUT, SP_ERR_STATE, SP_PENDING = 5, 6, 7, 8, 9, 10
+ELL_ERR_CUDA = 5
+SP_ID_MATRIX, SP_ID_FIBER = 0, 1
+SP_PREC_MIXED, SP_PREC_FP64 = 0, 1
+SP_MAX_RHS = 8
+MAX_ITS, MIN_ERR = 100000, 1.0e-10
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_up = C.POINTER(C.c_ubyte)
+_vp = C.c_void_p
+
+
+class SputnikError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+# ------------------------------------------------------------------ structs ---
+
+class ell_matrix(C.Structure):
+    _fields_ = [("nrow", C.c_int), ("ncol", C.c_int), ("nnz", C.c_int), ("cols", _ip),
+                ("vals", _dp)]
+
+
+class ell_solver(C.Structure):
+    _fields_ = [("max_its", C.c_int), ("its", C.c_int), ("min_err", C.c_double),
+                ("err", C.c_double)]
+
+
+class sp_rve_desc(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("len", C.c_double * 3), ("nx_fib", C.c_int),
+                ("ny_fib", C.c_int), ("radius", C.c_double), ("desv", C.c_double * 2),
+                ("E", C.c_double * 2), ("nu", C.c_double * 2)]
+
+
+class sp_solve_info(C.Structure):
+    _fields_ = [("status", C.c_int), ("outer_its", C.c_int), ("inner_its", C.c_int),
+                ("pad", C.c_int), ("relres", C.c_double)]
+
+
+class sp_batch_opts(C.Structure):
+    _fields_ = [("nrhs", C.c_int), ("precision", C.c_int), ("rtol", C.c_double),
+                ("inner_rtol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
+                ("threads", C.c_int), ("lanes_per_row", C.c_int), ("ctas_per_sm", C.c_int),
+                ("pad", C.c_int)]
+
+
+class sp_server_opts(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_inflight", C.c_int),
+                ("queue_capacity", C.c_int), ("rtol", C.c_double), ("inner_rtol", C.c_double),
+                ("idle_spin_limit", C.c_int), ("pad", C.c_int)]
+
+
+# ------------------------------------------------------------------- loader ---
+
+# name -> (restype, argtypes); every symbol the public headers declare
+_PROTOS = {
+    # ell.h
+    "ell_init": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_int, C.c_int]),
+    "ell_set_val": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_int, C.c_double]),
+    "ell_add_val": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_int, C.c_double]),
+    "ell_add_vals": (C.c_int, [C.POINTER(ell_matrix), _ip, C.c_int, _ip, C.c_int, _dp]),
+    "ell_mvp": (C.c_int, [C.POINTER(ell_matrix), _dp, _dp]),
+    "ell_get_val": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_int, _dp]),
+    "ell_solve_jacobi": (C.c_int, [C.POINTER(ell_solver), C.POINTER(ell_matrix), _dp, _dp]),
+    "ell_set_zero_row": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_double]),
+    "ell_set_zero_col": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_double]),
+    "ell_set_zero_mat": (C.c_int, [C.POINTER(ell_matrix)]),
+    "ell_print_full": (C.c_int, [C.POINTER(ell_matrix)]),
+    # fem.h
+    "fem_init": (C.c_int, []),
+    "fem_init_struct": (C.c_int, [_vp, _vp, _vp, _dp, C.c_int]),
+    "fem_invjac": (C.c_int, [C.c_int, _vp, _vp, _dp]),
+    "fem_calc_jac": (C.c_int, [C.c_int, C.c_int, C.c_int, _dp, _vp, _vp]),
+    "fem_trans_dsh": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "fem_get_dsh_master": (C.c_int, [C.c_int, C.c_int, _vp]),
+    "fem_get_sh": (C.c_int, [C.c_int, C.c_int, _vp]),
+    "fem_get_wp": (C.c_int, [C.c_int, C.c_int, _vp]),
+    # sputnik_b200.h
+    "sp_last_error": (C.c_char_p, []),
+    "sp_version": (C.c_int, []),
+    "sp_init": (C.c_int, [C.c_int]),
+    "sp_device_count": (C.c_int, []),
+    "ell_set_zero_col_full": (C.c_int, [C.POINTER(ell_matrix), C.c_int, C.c_double]),
+    "ell_free": (C.c_int, [C.POINTER(ell_matrix)]),
+    "sp_ell_upload": (C.c_int, [C.POINTER(ell_matrix), C.POINTER(_vp)]),
+    "sp_ell_dev_free": (C.c_int, [_vp]),
+    "sp_ell_dev_mvp": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "sp_ell_dev_mvp_host": (C.c_int, [_vp, _dp, _dp]),
+    "sp_ell_dev_pcg": (C.c_int, [_vp, _dp, _dp, C.c_double, C.c_int, _ip, _dp]),
+    "sp_classify": (C.c_int, [C.POINTER(sp_rve_desc), _up]),
+    "sp_ell_pattern": (C.c_int, [_ip, _ip]),
+    "sp_rve_create": (C.c_int, [C.POINTER(sp_rve_desc), C.POINTER(_vp)]),
+    "sp_rve_destroy": (C.c_int, [_vp]),
+    "sp_rve_sizes": (C.c_int, [_vp, _ip, _ip, _ip]),
+    "sp_rve_get_ell": (C.c_int, [_vp, _ip, _dp]),
+    "sp_rve_get_ke": (C.c_int, [_vp, _dp, _dp]),
+    "sp_rve_homogenize": (C.c_int, [_vp, C.c_int, _dp, C.c_double, _dp, _dp, _dp,
+                                    C.POINTER(sp_solve_info)]),
+    "sp_rve_tangent": (C.c_int, [_vp, C.c_double, _dp, C.POINTER(sp_solve_info)]),
+    "sp_batch_opts_default": (None, [C.POINTER(sp_batch_opts)]),
+    "sp_batch_create": (C.c_int, [C.c_int, C.POINTER(sp_rve_desc), C.POINTER(sp_batch_opts),
+                                  C.POINTER(_vp)]),
+    "sp_batch_destroy": (C.c_int, [_vp]),
+    "sp_batch_device_bytes": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "sp_batch_upload": (C.c_int, [_vp, _dp, _dp, _vp]),
+    "sp_batch_launch": (C.c_int, [_vp, _vp]),
+    "sp_batch_download": (C.c_int, [_vp, _dp, _dp, C.POINTER(sp_solve_info), _vp]),
+    "sp_batch_homogenize": (C.c_int, [_vp, _dp, _dp, _dp, _dp, C.POINTER(sp_solve_info), _vp]),
+    "sp_batch_last_launches": (C.c_int, [_vp, _ip]),
+    "sp_server_opts_default": (None, [C.POINTER(sp_server_opts)]),
+    "sp_server_create": (C.c_int, [C.c_int, C.POINTER(sp_rve_desc), C.POINTER(sp_server_opts),
+                                   C.POINTER(_vp)]),
+    "sp_server_destroy": (C.c_int, [_vp]),
+    "sp_server_plan_bytes": (C.c_int, [C.c_int, C.POINTER(sp_rve_desc),
+                                       C.POINTER(sp_server_opts), C.POINTER(C.c_size_t)]),
+    "sp_server_start": (C.c_int, [_vp]),
+    "sp_server_submit": (C.c_int, [_vp, C.c_int, _dp, C.POINTER(C.c_longlong)]),
+    "sp_server_poll": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.POINTER(sp_solve_info)]),
+    "sp_server_stop": (C.c_int, [_vp]),
+}
+
+# data symbols the headers declare (fem.h tables, solvers.h selector)
+DATA_SYMBOLS = [f"{k}_{e}" for e in ("segm_2", "tria_3", "quad_4", "tetra_4", "prism_6", "hexa_8")
+                for k in ("xp", "wp", "sh", "ds")] + ["solver"]
+
+_lib = None
+MISSING: list = []  # prototypes the loaded library does not export
+
+
+def load() -> C.CDLL:
+    """Load libsputnik_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built: run `python -m madmax_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            try:
+                f = getattr(L, name)
+            except AttributeError:
+                MISSING.append(name)
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def lib() -> C.CDLL:
+    return load()
+
+
+def last_error() -> str:
+    return (lib().sp_last_error() or b"").decode()
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0 and rc != SP_PENDING:
+        raise SputnikError(rc, f"{what}: {last_error()}")
+
+
+def device_count() -> int:
+    return lib().sp_device_count()
+
+
+def ptr(a: np.ndarray, t=_dp):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+# --------------------------------------------------------------- ELL (drop-in)
+
+class EllMatrix:
+    """Owns an ell_matrix built by the library's ell_init (host arrays)."""
+
+    def __init__(self, nrow: int, ncol: int, nnz: int):
+        self.m = ell_matrix()
+        check(lib().ell_init(C.byref(self.m), nrow, ncol, nnz), "ell_init")
+
+    @property
+    def cols(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.m.cols, shape=(self.m.nrow, self.m.nnz))
+
+    @property
+    def vals(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.m.vals, shape=(self.m.nrow, self.m.nnz))
+
+    def add_vals(self, ix, iy, vals) -> int:
+        ix = np.ascontiguousarray(ix, dtype=np.int32)
+        iy = np.ascontiguousarray(iy, dtype=np.int32)
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        return lib().ell_add_vals(C.byref(self.m), ptr(ix, _ip), len(ix), ptr(iy, _ip), len(iy),
+                                  ptr(v))
+
+    def mvp(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.m.nrow)
+        check(lib().ell_mvp(C.byref(self.m), ptr(x), ptr(y)), "ell_mvp")
+        return y
+
+    def solve_jacobi(self, b, x0):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x0, dtype=np.float64)
+        s = ell_solver()
+        check(lib().ell_solve_jacobi(C.byref(s), C.byref(self.m), ptr(b), ptr(x)),
+              "ell_solve_jacobi")
+        return x, s.its, s.err
+
+    def __del__(self):
+        try:
+            lib().ell_free(C.byref(self.m))
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------- RVE
+
+def rve_desc(n, radius=0.25, E=(1e9, 1e10), nu=(0.3, 0.2), length=1.0, nfib=(1, 1),
+             desv=(0.0, 0.0)) -> sp_rve_desc:
+    d = sp_rve_desc()
+    nn = (n, n, n) if np.isscalar(n) else tuple(n)
+    ll = (length,) * 3 if np.isscalar(length) else tuple(length)
+    for k in range(3):
+        d.n[k] = int(nn[k])
+        d.len[k] = float(ll[k])
+    d.nx_fib, d.ny_fib = nfib
+    d.radius = radius
+    d.desv[0], d.desv[1] = desv
+    d.E[0], d.E[1] = E
+    d.nu[0], d.nu[1] = nu
+    return d
+
+
+def classify(desc: sp_rve_desc) -> np.ndarray:
+    nelm = desc.n[0] * desc.n[1] * desc.n[2]
+    et = np.zeros(nelm, dtype=np.uint8)
+    check(lib().sp_classify(C.byref(desc), ptr(et, _up)), "sp_classify")
+    return et
+
+
+def ell_pattern(n) -> np.ndarray:
+    nn = np.array([n] * 3 if np.isscalar(n) else n, dtype=np.int32)
+    ndof = 3 * int(np.prod(nn + 1))
+    cols = np.zeros((ndof, 81), dtype=np.int32)
+    check(lib().sp_ell_pattern(ptr(nn, _ip), ptr(cols, _ip)), "sp_ell_pattern")
+    return cols
+
+
+class Rve:
+    """One RVE on the GPU (plain FP64 path)."""
+
+    def __init__(self, desc: sp_rve_desc):
+        self.desc = desc
+        self.h = _vp()
+        check(lib().sp_rve_create(C.byref(desc), C.byref(self.h)), "sp_rve_create")
+        nd, ne, nf = C.c_int(), C.c_int(), C.c_int()
+        check(lib().sp_rve_sizes(self.h, C.byref(nd), C.byref(ne), C.byref(nf)), "sp_rve_sizes")
+        self.ndof, self.nelm, self.nfiber = nd.value, ne.value, nf.value
+
+    def ell(self):
+        cols = np.zeros((self.ndof, 81), dtype=np.int32)
+        vals = np.zeros((self.ndof, 81))
+        check(lib().sp_rve_get_ell(self.h, ptr(cols, _ip), ptr(vals)), "sp_rve_get_ell")
+        return cols, vals
+
+    def ke(self):
+        a = np.zeros(576)
+        b = np.zeros(576)
+        check(lib().sp_rve_get_ke(self.h, ptr(a), ptr(b)), "sp_rve_get_ke")
+        return a.reshape(24, 24), b.reshape(24, 24)
+
+    def homogenize(self, strains, rtol=1e-8, want_u=False):
+        s = np.ascontiguousarray(np.atleast_2d(strains), dtype=np.float64)
+        k = s.shape[0]
+        sa = np.zeros((k, 6))
+        st = np.zeros((k, 6))
+        u = np.zeros((k, self.ndof)) if want_u else None
+        info = sp_solve_info()
+        check(lib().sp_rve_homogenize(self.h, k, ptr(s), rtol, ptr(sa), ptr(st), ptr(u),
+                                      C.byref(info)), "sp_rve_homogenize")
+        return sa, st, u, info
+
+    def tangent(self, rtol=1e-8):
+        Cm = np.zeros(36)
+        info = sp_solve_info()
+        check(lib().sp_rve_tangent(self.h, rtol, ptr(Cm), C.byref(info)), "sp_rve_tangent")
+        return Cm.reshape(6, 6), info
+
+    def close(self):
+        if self.h:
+            lib().sp_rve_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# -------------------------------------------------------------------- batch
+
+def batch_opts(**kw) -> sp_batch_opts:
+    o = sp_batch_opts()
+    lib().sp_batch_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Batch:
+    """Many RVEs solved by one persistent launch (mixed precision by default)."""
+
+    def __init__(self, descs, **opts):
+        self.n = len(descs)
+        self.descs = (sp_rve_desc * self.n)(*descs)
+        self.opts = batch_opts(**opts)
+        self.h = _vp()
+        check(lib().sp_batch_create(self.n, self.descs, C.byref(self.opts), C.byref(self.h)),
+              "sp_batch_create")
+        self.nrhs = self.opts.nrhs
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        check(lib().sp_batch_device_bytes(self.h, C.byref(b)), "sp_batch_device_bytes")
+        return b.value
+
+    def upload(self, strains=None, materials=None, stream=None):
+        check(lib().sp_batch_upload(self.h, ptr(strains), ptr(materials), stream),
+              "sp_batch_upload")
+
+    def launch(self, stream=None):
+        check(lib().sp_batch_launch(self.h, stream), "sp_batch_launch")
+
+    def download(self, stress=None, strain=None, info=None, stream=None):
+        check(lib().sp_batch_download(self.h, ptr(stress), ptr(strain), info, stream),
+              "sp_batch_download")
+
+    def homogenize(self, strains=None, materials=None, stream=None):
+        stress = np.zeros((self.n, self.nrhs, 6))
+        strain = np.zeros((self.n, self.nrhs, 6))
+        info = (sp_solve_info * self.n)()
+        check(lib().sp_batch_homogenize(self.h, ptr(strains), ptr(materials), ptr(stress),
+                                        ptr(strain), info, stream), "sp_batch_homogenize")
+        return stress, strain, info
+
+    def last_launches(self) -> int:
+        n = C.c_int()
+        check(lib().sp_batch_last_launches(self.h, C.byref(n)), "sp_batch_last_launches")
+        return n.value
+
+    def close(self):
+        if self.h:
+            lib().sp_batch_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def info_array(info) -> np.ndarray:
+    """sp_solve_info[] -> structured numpy view (status, outer, inner, relres)."""
+    return np.array([(i.status, i.outer_its, i.inner_its, i.relres) for i in info],
+                    dtype=[("status", "i4"), ("outer", "i4"), ("inner", "i4"), ("relres", "f8")])

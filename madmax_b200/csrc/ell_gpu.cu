@@ -1,0 +1,432 @@
+// ell_gpu.cu -- the compute half of the drop-in ell.h (ell_mvp,
+// ell_solve_jacobi) and the resident device ELL (sp_ell_dev_*).
+//
+// ell_mvp / ell_solve_jacobi take the caller's host matrix and vectors,
+// copy them to the GPU, compute there and copy the results back.  Their
+// arithmetic follows the reference's order exactly (per row, products
+// rounded separately and summed in slot order from 0, stopping at the first
+// empty slot; the Jacobi error summed over rows in row order), so results
+// are bit-identical to the reference's src/ell.c:127-184.
+#include <mutex>
+
+#include "ell.h"
+#include "pcg.cuh"
+#include "sp_cuda.h"
+
+namespace sp {
+
+// ----------------------------------------------------- exact-order SpMV ---
+
+// One warp per row.  Lane j forms the product of slot base+j; the running
+// sum is then extended in slot order with broadcast shuffles, so every lane
+// holds the reference's left-to-right sum.  Columns outside [0, ncol) other
+// than the -1 terminator are reported in *bad and skipped.
+__device__ inline double row_sum_exact(int row, int nnz, int ncol, const int *__restrict__ cols,
+                                       const double *__restrict__ vals, const double *__restrict__ x,
+                                       int lane, int *bad) {
+  double s = 0.0;
+  for (int base = 0; base < nnz; base += 32) {
+    int j = base + lane;
+    int c = (j < nnz) ? cols[(size_t)row * nnz + j] : -1;
+    unsigned stop = __ballot_sync(0xffffffffu, c == -1);
+    int first = stop ? __ffs(stop) - 1 : 32;
+    double p = 0.0;
+    if (lane < first) {
+      if (c < 0 || c >= ncol) {
+        atomicExch(bad, 1);
+      } else {
+        p = __dmul_rn(vals[(size_t)row * nnz + j], x[c]);
+      }
+    }
+    for (int q = 0; q < first; q++) s = __dadd_rn(s, __shfl_sync(0xffffffffu, p, q));
+    if (first < 32) break;
+  }
+  return s;
+}
+
+__global__ void k_mvp_exact(int nrow, int nnz, int ncol, const int *__restrict__ cols,
+                            const double *__restrict__ vals, const double *__restrict__ x,
+                            double *y, int *bad) {
+  int lane = threadIdx.x & 31;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int row = warp; row < nrow; row += nw) {
+    double s = row_sum_exact(row, nnz, ncol, cols, vals, x, lane, bad);
+    if (lane == 0) y[row] = s;
+  }
+}
+
+// ------------------------------------------------------- exact Jacobi ---
+
+struct JacobiState {
+  double err;
+  int its, max_its, done, pad;
+};
+
+// r_i = (A x)_i - b_i  (src/ell.c:163-167)
+__global__ void k_jacobi_resid(int nrow, int nnz, int ncol, const int *__restrict__ cols,
+                               const double *__restrict__ vals, const double *__restrict__ x,
+                               const double *__restrict__ b, double *r, int *bad,
+                               const JacobiState *st) {
+  if (st->done) return;
+  int lane = threadIdx.x & 31;
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int row = warp; row < nrow; row += nw) {
+    double s = row_sum_exact(row, nnz, ncol, cols, vals, x, lane, bad);
+    if (lane == 0) r[row] = __dsub_rn(s, b[row]);
+  }
+}
+
+// err = sqrt(sum_i r_i^2), summed in row order by one warp (lane 0 extends
+// the sum with the 32 squares of each coalesced chunk); stop when err < 1e-10
+__global__ void k_jacobi_err(int nrow, const double *__restrict__ r, JacobiState *st,
+                             double min_err, cudaGraphConditionalHandle h) {
+  if (st->done) return;
+  int lane = threadIdx.x;
+  double s = 0.0;
+  for (int base = 0; base < nrow; base += 32) {
+    double v = (base + lane < nrow) ? r[base + lane] : 0.0;
+    double sq = __dmul_rn(v, v);
+    int cnt = min(32, nrow - base);
+    for (int q = 0; q < cnt; q++) s = __dadd_rn(s, __shfl_sync(0xffffffffu, sq, q));
+  }
+  if (lane == 0) {
+    double err = __dsqrt_rn(s);
+    st->err = err;
+    if (err < min_err) {
+      st->done = 1;
+      cudaGraphSetConditional(h, 0);
+    }
+  }
+}
+
+// x_i -= dinv_i * r_i; its++  (src/ell.c:169-177)
+__global__ void k_jacobi_update(int nrow, const double *__restrict__ dinv,
+                                const double *__restrict__ r, double *x, JacobiState *st,
+                                cudaGraphConditionalHandle h) {
+  if (st->done) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  for (int i = t; i < nrow; i += nt) x[i] = __dsub_rn(x[i], __dmul_rn(dinv[i], r[i]));
+  if (t == 0) {
+    int its = st->its + 1;
+    st->its = its;
+    if (its >= st->max_its) cudaGraphSetConditional(h, 0);
+  }
+}
+
+// ----------------------------------------------- scratch for host calls ---
+
+struct Scratch {
+  void *p = nullptr;
+  size_t cap = 0;
+  int get(size_t bytes, void **out) {
+    if (bytes > cap) {
+      if (p) cudaFree(p);
+      p = nullptr;
+      cap = 0;
+      SP_TRY(dmalloc(&p, bytes, nullptr));
+      cap = bytes;
+    }
+    *out = p;
+    return SP_OK;
+  }
+};
+static std::mutex g_ell_mu;
+static Scratch g_ell_scratch[64];
+
+static int launch_blocks(Device *d, long long warps_needed) {
+  long long b = (warps_needed + 7) / 8;
+  long long cap = (long long)d->nsm * 8;
+  if (b < 1) b = 1;
+  return (int)(b < cap ? b : cap);
+}
+
+}  // namespace sp
+
+using namespace sp;
+
+extern "C" int ell_mvp(ell_matrix *m, double *x, double *y) {
+  if (m == NULL || x == NULL || y == NULL) return 1;
+  if (m->nrow <= 0) return 0;
+  Device *d;
+  if (device(&d)) return ELL_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_ell_mu);
+  size_t ns = (size_t)m->nrow * m->nnz;
+  size_t bc = ns * sizeof(int), bv = ns * sizeof(double), bx = (size_t)m->ncol * sizeof(double),
+         by = (size_t)m->nrow * sizeof(double);
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  char *base;
+  if (g_ell_scratch[d->id].get(al(bc) + al(bv) + al(bx) + al(by) + 256, (void **)&base))
+    return ELL_ERR_CUDA;
+  int *dc = (int *)base;
+  double *dv = (double *)(base + al(bc));
+  double *dx = (double *)(base + al(bc) + al(bv));
+  double *dy = (double *)(base + al(bc) + al(bv) + al(bx));
+  int *dbad = (int *)(base + al(bc) + al(bv) + al(bx) + al(by));
+  cudaStream_t s = d->stream;
+  int bad = 0;
+  if (cudaMemcpyAsync(dc, m->cols, bc, cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(dv, m->vals, bv, cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(dx, x, bx, cudaMemcpyHostToDevice, s) ||
+      cudaMemsetAsync(dbad, 0, sizeof(int), s))
+    return sp_set_error(ELL_ERR_CUDA, "ell_mvp: copy to device failed");
+  k_mvp_exact<<<launch_blocks(d, m->nrow), 256, 0, s>>>(m->nrow, m->nnz, m->ncol, dc, dv, dx, dy,
+                                                         dbad);
+  if (cudaGetLastError() || cudaMemcpyAsync(y, dy, by, cudaMemcpyDeviceToHost, s) ||
+      cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s) ||
+      cudaStreamSynchronize(s))
+    return sp_set_error(ELL_ERR_CUDA, "ell_mvp: kernel or copy failed");
+  if (bad) return sp_set_error(1, "ell_mvp: column index outside [0, ncol)");
+  return 0;
+}
+
+extern "C" int ell_solve_jacobi(ell_solver *solver, ell_matrix *m, double *b, double *x) {
+  if (m == NULL || b == NULL || x == NULL) return 1;
+  if (m->nrow <= 0) {
+    solver->its = 0;
+    solver->err = 0.0;
+    return 0;
+  }
+  Device *d;
+  if (device(&d)) return ELL_ERR_CUDA;
+  // k_diag_inv(i) = 1 / m(i,i) with ell_get_val's lookup (src/ell.c:150-154)
+  double *dinv_h = (double *)malloc((size_t)m->nrow * sizeof(double));
+  if (!dinv_h) return 2;
+  for (int i = 0; i < m->nrow; i++) {
+    double v = 0.0;
+    if (i < m->ncol) ell_get_val(m, i, i, &v);
+    dinv_h[i] = 1 / v;
+  }
+  std::lock_guard<std::mutex> lk(g_ell_mu);
+  size_t ns = (size_t)m->nrow * m->nnz;
+  // x is read at columns < ncol and written at rows < nrow (one array in
+  // the reference): size it for both
+  size_t nx = (size_t)(m->nrow > m->ncol ? m->nrow : m->ncol);
+  size_t bc = ns * sizeof(int), bv = ns * sizeof(double), bx = nx * sizeof(double),
+         bn = (size_t)m->nrow * sizeof(double);
+  auto al = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  char *base;
+  if (g_ell_scratch[d->id].get(al(bc) + al(bv) + al(bx) + 3 * al(bn) + 512, (void **)&base)) {
+    free(dinv_h);
+    return ELL_ERR_CUDA;
+  }
+  int *dc = (int *)base;
+  double *dv = (double *)(base + al(bc));
+  double *dx = (double *)(base + al(bc) + al(bv));
+  double *db = (double *)(base + al(bc) + al(bv) + al(bx));
+  double *dr = db + al(bn) / sizeof(double);
+  double *dd = dr + al(bn) / sizeof(double);
+  int *dbad = (int *)(dd + al(bn) / sizeof(double));
+  JacobiState *dst = (JacobiState *)(dbad + 64);
+  JacobiState st0 = {0.0, 0, MAX_ITS, 0, 0};
+  cudaStream_t s = d->stream;
+  int rc = 0;
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  do {
+    if (cudaMemcpyAsync(dc, m->cols, bc, cudaMemcpyHostToDevice, s) ||
+        cudaMemcpyAsync(dv, m->vals, bv, cudaMemcpyHostToDevice, s) ||
+        cudaMemcpyAsync(dx, x, bx, cudaMemcpyHostToDevice, s) ||
+        cudaMemcpyAsync(db, b, bn, cudaMemcpyHostToDevice, s) ||
+        cudaMemcpyAsync(dd, dinv_h, bn, cudaMemcpyHostToDevice, s) ||
+        cudaMemcpyAsync(dst, &st0, sizeof(st0), cudaMemcpyHostToDevice, s) ||
+        cudaMemsetAsync(dbad, 0, sizeof(int), s)) {
+      rc = sp_set_error(ELL_ERR_CUDA, "ell_solve_jacobi: copy to device failed");
+      break;
+    }
+    cudaGraphConditionalHandle h;
+    if (cudaGraphCreate(&g, 0) || cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault)) {
+      rc = sp_set_error(ELL_ERR_CUDA, "ell_solve_jacobi: graph creation failed");
+      break;
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    if (cudaGraphAddNode(&wn, g, nullptr, 0, &cp)) {
+      rc = sp_set_error(ELL_ERR_CUDA, "ell_solve_jacobi: conditional node failed");
+      break;
+    }
+    cudaGraph_t body = cp.conditional.phGraph_out[0], cap;
+    int nb = launch_blocks(d, m->nrow);
+    if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal)) {
+      rc = sp_set_error(ELL_ERR_CUDA, "ell_solve_jacobi: capture failed");
+      break;
+    }
+    k_jacobi_resid<<<nb, 256, 0, s>>>(m->nrow, m->nnz, m->ncol, dc, dv, dx, db, dr, dbad, dst);
+    k_jacobi_err<<<1, 32, 0, s>>>(m->nrow, dr, dst, MIN_ERR, h);
+    k_jacobi_update<<<nb, 256, 0, s>>>(m->nrow, dd, dr, dx, dst, h);
+    if (cudaStreamEndCapture(s, &cap) || cudaGraphInstantiate(&ge, g, 0) ||
+        cudaGraphLaunch(ge, s)) {
+      rc = sp_set_error(ELL_ERR_CUDA, "ell_solve_jacobi: graph launch failed");
+      break;
+    }
+    JacobiState st;
+    int bad = 0;
+    if (cudaMemcpyAsync(x, dx, bn, cudaMemcpyDeviceToHost, s) ||
+        cudaMemcpyAsync(&st, dst, sizeof(st), cudaMemcpyDeviceToHost, s) ||
+        cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s) ||
+        cudaStreamSynchronize(s)) {
+      rc = sp_set_error(ELL_ERR_CUDA, "ell_solve_jacobi: kernel or copy failed");
+      break;
+    }
+    if (bad) {
+      rc = sp_set_error(1, "ell_solve_jacobi: column index outside [0, ncol)");
+      break;
+    }
+    solver->err = st.err;
+    solver->its = st.its;
+  } while (0);
+  if (ge) cudaGraphExecDestroy(ge);
+  if (g) cudaGraphDestroy(g);
+  free(dinv_h);
+  return rc;
+}
+
+// --------------------------------------------------- resident device ELL ---
+
+struct sp_ell_dev_s {
+  int nrow, ncol, nnz, wp, dev;
+  int *cols = nullptr;    // [nrow][wp]
+  double *vals = nullptr; // [nrow][wp]
+  double *dinv = nullptr;
+  double *vec = nullptr;  // 5 vectors of nrow + x of ncol
+  PcgState *st = nullptr;
+  double *partial = nullptr;
+  unsigned *ticket = nullptr;
+  PcgGraph<double, 1, 32> *pcg = nullptr;
+};
+
+extern "C" int sp_ell_upload(const ell_matrix *m, sp_ell_dev **out) {
+  if (!m || !out || m->nrow <= 0 || m->nnz <= 0 || !m->cols || !m->vals)
+    return sp_set_error(SP_ERR_ARG, "sp_ell_upload: bad matrix");
+  if (m->ncol != m->nrow) return sp_set_error(SP_ERR_ARG, "sp_ell_upload: matrix must be square");
+  for (size_t i = 0; i < (size_t)m->nrow * m->nnz; i++)
+    if (m->cols[i] < -1 || m->cols[i] >= m->ncol)
+      return sp_set_error(SP_ERR_RANGE, "sp_ell_upload: column index outside the matrix");
+  Device *d;
+  SP_TRY(device(&d));
+  sp_ell_dev *a = new sp_ell_dev_s();
+  a->nrow = m->nrow;
+  a->ncol = m->ncol;
+  a->nnz = m->nnz;
+  a->wp = (m->nnz + 3) / 4 * 4;
+  a->dev = d->id;
+  size_t nslot = (size_t)a->nrow * a->wp;
+  int *hc = (int *)malloc(nslot * sizeof(int));
+  double *hv = (double *)malloc(nslot * sizeof(double));
+  double *hd = (double *)malloc(a->nrow * sizeof(double));
+  int rc = (!hc || !hv || !hd) ? sp_set_error(SP_ERR_NOMEM, "host staging") : SP_OK;
+  if (!rc) {
+    for (int r = 0; r < a->nrow; r++) {
+      bool ended = false;
+      double diag = 0.0;
+      for (int j = 0; j < a->wp; j++) {
+        int c = (j < m->nnz && !ended) ? m->cols[(size_t)r * m->nnz + j] : -1;
+        if (c == -1) ended = true;
+        hc[(size_t)r * a->wp + j] = c;
+        hv[(size_t)r * a->wp + j] = (c >= 0) ? m->vals[(size_t)r * m->nnz + j] : 0.0;
+        if (c == r) diag = hv[(size_t)r * a->wp + j];
+      }
+      hd[r] = 1.0 / diag;
+    }
+    rc = dmalloc((void **)&a->cols, nslot * sizeof(int), nullptr);
+    if (!rc) rc = dmalloc((void **)&a->vals, nslot * sizeof(double), nullptr);
+    if (!rc) rc = dmalloc((void **)&a->dinv, a->nrow * sizeof(double), nullptr);
+    if (!rc) rc = dmalloc((void **)&a->vec, 6 * (size_t)a->nrow * sizeof(double), nullptr);
+    if (!rc) rc = dmalloc((void **)&a->st, sizeof(PcgState), nullptr);
+    if (!rc) rc = dmalloc((void **)&a->partial, 4096 * 2 * sizeof(double), nullptr);
+    if (!rc) rc = dmalloc((void **)&a->ticket, 64, nullptr);
+    if (!rc && (cudaMemcpy(a->cols, hc, nslot * sizeof(int), cudaMemcpyHostToDevice) ||
+                cudaMemcpy(a->vals, hv, nslot * sizeof(double), cudaMemcpyHostToDevice) ||
+                cudaMemcpy(a->dinv, hd, a->nrow * sizeof(double), cudaMemcpyHostToDevice) ||
+                cudaMemset(a->ticket, 0, 64)))
+      rc = sp_set_error(SP_ERR_CUDA, "sp_ell_upload: copy failed");
+  }
+  free(hc);
+  free(hv);
+  free(hd);
+  if (rc) {
+    sp_ell_dev_free(a);
+    return rc;
+  }
+  *out = a;
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_free(sp_ell_dev *a) {
+  if (!a) return SP_OK;
+  delete a->pcg;
+  cudaFree(a->cols);
+  cudaFree(a->vals);
+  cudaFree(a->dinv);
+  cudaFree(a->vec);
+  cudaFree(a->st);
+  cudaFree(a->partial);
+  cudaFree(a->ticket);
+  delete a;
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_mvp(sp_ell_dev *a, const double *x_dev, double *y_dev, void *stream) {
+  if (!a || !x_dev || !y_dev) return sp_set_error(SP_ERR_ARG, "sp_ell_dev_mvp: null argument");
+  Device *d;
+  SP_TRY(device(&d));
+  cudaStream_t s = pick_stream(stream, d);
+  int nb = launch_blocks(d, a->nrow);
+  k_spmm_plain<double, 1, 32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->wp, a->vals, a->cols, x_dev,
+                                                         y_dev);
+  SP_CUDA_TRY(cudaGetLastError());
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_mvp_host(sp_ell_dev *a, const double *x, double *y) {
+  if (!a || !x || !y) return sp_set_error(SP_ERR_ARG, "sp_ell_dev_mvp_host: null argument");
+  Device *d;
+  SP_TRY(device(&d));
+  double *dx = a->vec, *dy = a->vec + a->nrow;
+  size_t bn = (size_t)a->nrow * sizeof(double);
+  SP_CUDA_TRY(cudaMemcpyAsync(dx, x, bn, cudaMemcpyHostToDevice, d->stream));
+  SP_TRY(sp_ell_dev_mvp(a, dx, dy, d->stream));
+  SP_CUDA_TRY(cudaMemcpyAsync(y, dy, bn, cudaMemcpyDeviceToHost, d->stream));
+  SP_CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_pcg(sp_ell_dev *a, const double *b, double *x, double rtol, int max_its,
+                              int *its, double *relres) {
+  if (!a || !b || !x) return sp_set_error(SP_ERR_ARG, "sp_ell_dev_pcg: null argument");
+  Device *d;
+  SP_TRY(device(&d));
+  cudaStream_t s = d->stream;
+  size_t n = a->nrow, bn = n * sizeof(double);
+  double *vb = a->vec, *vx = vb + n, *vr = vx + n, *vp = vr + n, *vq = vp + n;
+  int nb = launch_blocks(d, a->nrow);
+  if (nb > 4096) nb = 4096;
+  if (!a->pcg) {
+    a->pcg = new PcgGraph<double, 1, 32>();
+    SP_TRY(a->pcg->build(s, nb, a->nrow, a->wp, a->vals, a->cols, a->dinv, vb, vx, vr, vp, vq, 0,
+                         a->st, a->partial, a->ticket));
+  }
+  PcgState st0 = {};
+  st0.nactive = 1;
+  st0.rtol2 = rtol * rtol;
+  st0.max_its = max_its;
+  SP_CUDA_TRY(cudaMemcpyAsync(vb, b, bn, cudaMemcpyHostToDevice, s));
+  SP_CUDA_TRY(cudaMemcpyAsync(vx, x, bn, cudaMemcpyHostToDevice, s));
+  SP_CUDA_TRY(cudaMemcpyAsync(a->st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+  SP_TRY(a->pcg->run(s, nullptr));
+  PcgState st;
+  SP_CUDA_TRY(cudaMemcpyAsync(x, vx, bn, cudaMemcpyDeviceToHost, s));
+  SP_CUDA_TRY(cudaMemcpyAsync(&st, a->st, sizeof(st), cudaMemcpyDeviceToHost, s));
+  SP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (its) *its = st.its;
+  if (relres) *relres = (st.bb[0] > 0) ? sqrt(st.rr[0] / st.bb[0]) : 0.0;
+  return st.active[0] ? sp_set_error(SP_ERR_NOCONV, "sp_ell_dev_pcg: no convergence in %d its",
+                                     st.its)
+                      : SP_OK;
+}

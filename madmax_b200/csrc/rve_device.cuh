@@ -1,0 +1,507 @@
+// rve_device.cuh -- device building blocks of the micro-RVE hot path, shared
+// by the plain one-RVE path (rve_plain.cu), the batched persistent kernel
+// (rve_batch.cu) and the serving loop (serve.cu).
+//
+// Every routine is written for a cooperating group of `nt` threads with
+// index `t` (a whole grid, or one CTA); the caller places the barriers.
+//
+// Layouts
+//   ELL values/cols : [ndof][SP_WP] row-major, 84 slots (81 used), -1 cols
+//                     and 0 values in unused slots.
+//   vectors         : [ndof][K] (the K load cases of one dof adjacent).
+//   Ke              : [type][24][24] row-major, i = 3*local_node + d.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sp_internal.h"
+
+namespace sp {
+
+struct MeshGeo {
+  int nx, ny, nz;    // nodes per axis
+  int nex, ney, nez; // elements per axis
+  int ndof, nelm;
+  double hx, hy, hz; // element edge lengths
+  double vol;        // RVE volume
+};
+
+__host__ __device__ inline bool is_bnode(const MeshGeo &g, int node) {
+  int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+  return i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1;
+}
+
+// hexa8 local node a -> corner offset (bit0 x, bit1 y, bit2 z), from the node
+// order of src/fem.c:324-362 (0:---, 1:+--, 2:++-, 3:-+-, 4..7 same at z+)
+__host__ __device__ inline int corner_x(int a) { return ((a & 3) == 1 || (a & 3) == 2) ? 1 : 0; }
+__host__ __device__ inline int corner_y(int a) { return ((a & 3) >= 2) ? 1 : 0; }
+__host__ __device__ inline int corner_z(int a) { return a >> 2; }
+
+__device__ inline void elem_nodes(const MeshGeo &g, int e, int *nod) {
+  int ex = e % g.nex, ey = (e / g.nex) % g.ney, ez = e / (g.nex * g.ney);
+  int nxy = g.nx * g.ny;
+  int n0 = ex + ey * g.nx + ez * nxy;
+  nod[0] = n0;
+  nod[1] = n0 + 1;
+  nod[2] = n0 + g.nx + 1;
+  nod[3] = n0 + g.nx;
+#pragma unroll
+  for (int a = 0; a < 4; a++) nod[4 + a] = nod[a] + nxy;
+}
+
+// exact (separately rounded) double arithmetic, matching the oracle's
+// -ffp-contract=off build bit for bit
+__device__ inline double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ inline double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ inline double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// ------------------------------------------------------------- materials ---
+
+// 3D isotropic D in Voigt (xx,yy,zz,xy,yz,xz) from E, nu, with the Lame
+// constants of src/material.c:121-122
+__device__ inline void iso_D(double E, double nu, double *D) {
+  double lam = __ddiv_rn(dmul(E, nu), dmul(dadd(1.0, nu), dsub(1.0, dmul(2.0, nu))));
+  double mu = __ddiv_rn(E, dmul(2.0, dadd(1.0, nu)));
+  for (int i = 0; i < 36; i++) D[i] = 0.0;
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++) D[i * 6 + j] = lam;
+    D[i * 6 + i] = dadd(lam, dmul(2.0, mu));
+    D[(3 + i) * 6 + (3 + i)] = mu;
+  }
+}
+
+// ------------------------------------------------------ element operators ---
+
+#define SP_GP 0.577350269189626
+
+// dsh[a][d][gp] = dN_a/dxi_d(gp) * 2/h_d (src/fem.c:3-59 extended to 3D with
+// the hexa8 tables of src/fem.c:309-405); 192 entries
+__device__ inline double dsh_entry(int a, int d, int gp, const double h[3]) {
+  int s[3] = {corner_x(a) ? 1 : -1, corner_y(a) ? 1 : -1, corner_z(a) ? 1 : -1};
+  int q[3] = {corner_x(gp) ? 1 : -1, corner_y(gp) ? 1 : -1, corner_z(gp) ? 1 : -1};
+  double f[3];
+  for (int e = 0; e < 3; e++) {
+    double x = q[e] * SP_GP;
+    f[e] = (s[e] < 0) ? dsub(1.0, x) : dadd(1.0, x);
+  }
+  double v = s[d] * 1.0;
+  for (int e = 0; e < 3; e++)
+    if (e != d) v = dmul(v, f[e]);
+  v = dmul(v, 0.125);
+  return __ddiv_rn(dmul(v, 2.0), h[d]);
+}
+
+// B[v][i] at one Gauss point from dsh (micro/src/init.c:40-51 extended to 3D)
+__device__ inline double bmat_entry(const double *dsh, int v, int i, int gp) {
+  int a = i / 3, c = i % 3;
+  const double *da = dsh + a * 24; // [d][gp]
+  switch (v) {
+    case 0: return c == 0 ? da[0 * 8 + gp] : 0.0;
+    case 1: return c == 1 ? da[1 * 8 + gp] : 0.0;
+    case 2: return c == 2 ? da[2 * 8 + gp] : 0.0;
+    case 3: return c == 0 ? da[1 * 8 + gp] : (c == 1 ? da[0 * 8 + gp] : 0.0);
+    case 4: return c == 1 ? da[2 * 8 + gp] : (c == 2 ? da[1 * 8 + gp] : 0.0);
+    default: return c == 0 ? da[2 * 8 + gp] : (c == 2 ? da[0 * 8 + gp] : 0.0);
+  }
+}
+
+// Group-cooperative set-up of the element operators for ntype materials:
+//   dsh[192], Ke[t][576] = sum_gp B^T D_t B w (micro/src/assembly.c:97-108,
+//   same summation order, terms with a zero factor skipped, which leaves the
+//   sum unchanged), Bbar[6][24] = sum_gp w B(gp).
+// Needs a barrier between the two calls.
+__device__ inline void elem_ops_stage1(int t, int nt, const double h[3], double *dsh) {
+  for (int x = t; x < 192; x += nt) {
+    int a = x / 24, d = (x / 8) % 3, gp = x % 8;
+    dsh[x] = dsh_entry(a, d, gp, h);
+  }
+}
+
+__device__ inline void elem_ops_stage2(int t, int nt, const double h[3], const double *dsh,
+                                       const double *D /*[ntype][36]*/, int ntype,
+                                       double *Ke /*[ntype][576]*/, double *Bbar /*[144]*/) {
+  double w = __ddiv_rn(dmul(dmul(h[0], h[1]), h[2]), 8.0);
+  for (int x = t; x < ntype * SP_KE; x += nt) {
+    int ty = x / SP_KE, ij = x % SP_KE, i = ij / SP_NC, j = ij % SP_NC;
+    const double *C = D + ty * 36;
+    double s = 0.0;
+    for (int gp = 0; gp < 8; gp++) {
+      for (int k = 0; k < 6; k++) {
+        double bkj = bmat_entry(dsh, k, j, gp);
+        if (bkj == 0.0) continue;
+        for (int hh = 0; hh < 6; hh++) {
+          double bhi = bmat_entry(dsh, hh, i, gp);
+          double c = C[hh * 6 + k];
+          if (bhi == 0.0 || c == 0.0) continue;
+          s = dadd(s, dmul(dmul(dmul(bhi, c), bkj), w));
+        }
+      }
+    }
+    Ke[x] = s;
+  }
+  if (Bbar) {
+    for (int x = t; x < 144; x += nt) {
+      int v = x / 24, i = x % 24;
+      double s = 0.0;
+      for (int gp = 0; gp < 8; gp++) s = dadd(s, dmul(bmat_entry(dsh, v, i, gp), w));
+      Bbar[x] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------- assembly ---
+
+// Zero the values of an ELL matrix (ndof rows of SP_WP slots).
+template <typename T>
+__device__ inline void ell_zero(int t, int nt, T *vals, int ndof) {
+  size_t n = (size_t)ndof * SP_WP;
+  if (sizeof(T) == 4) {
+    float4 *v4 = reinterpret_cast<float4 *>(vals);
+    for (size_t x = t; x < n / 4; x += nt) v4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
+  } else {
+    double2 *v2 = reinterpret_cast<double2 *>(vals);
+    for (size_t x = t; x < n / 2; x += nt) v2[x] = make_double2(0.0, 0.0);
+  }
+}
+
+// One colour of the conflict-free scatter: for every element e of the colour
+// and every (i, j), vals[dof(e,i)][slot(e,i,j)] += Ke[type(e)][i][j].
+// Elements of one colour (same parity of ex, ey, ez) share no node, so the
+// work items of one colour write pairwise distinct slots; colours run in a
+// fixed order, so the sums are deterministic.
+template <typename T>
+__device__ inline void scatter_colour(int t, int nt, const MeshGeo &g, const int *color_elems,
+                                      int c0, int c1, const uint8_t *__restrict__ slot,
+                                      const uint8_t *__restrict__ etype, const T *Ke /*[2][576]*/,
+                                      T *vals) {
+  int nwork = (c1 - c0) * SP_KE;
+  for (int x = t; x < nwork; x += nt) {
+    int e = color_elems[c0 + x / SP_KE];
+    int ij = x % SP_KE;
+    int i = ij / SP_NC;
+    int nod[8];
+    elem_nodes(g, e, nod);
+    int row = nod[i / 3] * 3 + i % 3;
+    int s = slot[(size_t)e * SP_KE + ij];
+    vals[(size_t)row * SP_WP + s] += Ke[etype[e] * SP_KE + ij];
+  }
+}
+
+// Dirichlet rows and columns of every boundary dof (micro/src/assembly.c:
+// 112-135, the column cleared in every row) and the Jacobi diagonal inverse.
+template <typename T>
+__device__ inline void bc_and_dinv(int t, int nt, const MeshGeo &g, const int *__restrict__ cols,
+                                   T *vals, T *dinv) {
+  for (int row = t; row < g.ndof; row += nt) {
+    bool brow = is_bnode(g, row / 3);
+    const int *c = cols + (size_t)row * SP_WP;
+    T *v = vals + (size_t)row * SP_WP;
+    T diag = 0;
+    for (int s = 0; s < SP_ELL_WIDTH; s++) {
+      int col = c[s];
+      if (col < 0) break;
+      if (brow)
+        v[s] = (col == row) ? T(1) : T(0);
+      else if (is_bnode(g, col / 3))
+        v[s] = T(0);
+      if (col == row) diag = v[s];
+    }
+    dinv[row] = T(1) / diag;
+  }
+}
+
+// ------------------------------------------------------------ load cases ---
+
+// u = eps . x on boundary dofs (micro/src/homogenize.c:227-242, 335-342 in
+// 3D), zero elsewhere; eps[k][6] Voigt with engineering shears.
+template <int K>
+__device__ inline void affine_init(int t, int nt, const MeshGeo &g, const double *eps, int nrhs,
+                                   double *u) {
+  for (int x = t; x < g.ndof * K; x += nt) {
+    int dof = x / K, k = x % K;
+    int node = dof / 3, d = dof % 3;
+    double val = 0.0;
+    if (k < nrhs && is_bnode(g, node)) {
+      int i = node % g.nx, j = (node / g.nx) % g.ny, kk = node / (g.nx * g.ny);
+      double X = i * g.hx, Y = j * g.hy, Z = kk * g.hz;
+      const double *e = eps + k * 6;
+      if (d == 0)
+        val = dadd(dadd(dmul(e[0], X), dmul(e[3] / 2, Y)), dmul(e[5] / 2, Z));
+      else if (d == 1)
+        val = dadd(dadd(dmul(e[3] / 2, X), dmul(e[1], Y)), dmul(e[4] / 2, Z));
+      else
+        val = dadd(dadd(dmul(e[5] / 2, X), dmul(e[4] / 2, Y)), dmul(e[2], Z));
+    }
+    u[x] = val;
+  }
+}
+
+// Keep the interior of a warm start, overwrite the boundary with eps . x.
+template <int K>
+__device__ inline void affine_boundary(int t, int nt, const MeshGeo &g, const double *eps,
+                                       int nrhs, double *u) {
+  for (int x = t; x < g.ndof * K; x += nt) {
+    int dof = x / K, k = x % K;
+    int node = dof / 3, d = dof % 3;
+    if (!is_bnode(g, node)) {
+      if (k >= nrhs) u[x] = 0.0;
+      continue;
+    }
+    double val = 0.0;
+    if (k < nrhs) {
+      int i = node % g.nx, j = (node / g.nx) % g.ny, kk = node / (g.nx * g.ny);
+      double X = i * g.hx, Y = j * g.hy, Z = kk * g.hz;
+      const double *e = eps + k * 6;
+      if (d == 0)
+        val = dadd(dadd(dmul(e[0], X), dmul(e[3] / 2, Y)), dmul(e[5] / 2, Z));
+      else if (d == 1)
+        val = dadd(dadd(dmul(e[3] / 2, X), dmul(e[1], Y)), dmul(e[4] / 2, Z));
+      else
+        val = dadd(dadd(dmul(e[5] / 2, X), dmul(e[4] / 2, Y)), dmul(e[2], Z));
+    }
+    u[x] = val;
+  }
+}
+
+// ------------------------------------------------- FP64 element residual ---
+
+// Newton right-hand side b = -K u on interior dofs, 0 on boundary dofs
+// (micro/src/assembly.c:33-82 then negative_res, micro/src/homogenize.c:
+// 289-303): per node, the sum over its (up to 8) elements of Ke_t u_e.  For
+// linear elastic elements Ke_t u_e = sum_gp B^T sigma(B u_e) w exactly.
+// Writes b into rb (type R) and adds |b|^2 per load case into nrm2[K].
+template <int K, typename R>
+__device__ inline void residual_nodes(int t, int nt, const MeshGeo &g,
+                                      const uint8_t *__restrict__ etype,
+                                      const double *Ke /*[2][576], shared*/,
+                                      const double *__restrict__ u, R *rb, double *nrm2) {
+  int nn = g.ndof / 3;
+  for (int node = t; node < nn; node += nt) {
+    int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+    double acc[3][K];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int q = 0; q < K; q++) acc[d][q] = 0.0;
+    bool bnd = (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1);
+    if (!bnd) {
+      // interior node: all 8 surrounding elements exist
+      for (int c = 0; c < 8; c++) {
+        int ox = (c & 1), oy = (c >> 1) & 1, oz = c >> 2;
+        int ex = i - 1 + ox, ey = j - 1 + oy, ez = k - 1 + oz;
+        int e = ex + ey * g.nex + ez * g.nex * g.ney;
+        // local index of this node in element e: corner (1-ox, 1-oy, 1-oz)
+        int cx = 1 - ox, cy = 1 - oy, cz = 1 - oz;
+        int la = cz * 4 + ((cy == 0) ? (cx ? 1 : 0) : (cx ? 2 : 3));
+        const double *ke = Ke + etype[e] * SP_KE + (la * 3) * SP_NC;
+        int n0 = ex + ey * g.nx + ez * g.nx * g.ny;
+        for (int b = 0; b < 8; b++) {
+          int nb = n0 + corner_x(b) + corner_y(b) * g.nx + corner_z(b) * g.nx * g.ny;
+          const double *ub = u + (size_t)nb * 3 * K;
+#pragma unroll
+          for (int db = 0; db < 3; db++) {
+            double uv[K];
+#pragma unroll
+            for (int q = 0; q < K; q++) uv[q] = ub[db * K + q];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+              double kv = ke[d * SP_NC + b * 3 + db];
+#pragma unroll
+              for (int q = 0; q < K; q++) acc[d][q] = fma(kv, uv[q], acc[d][q]);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        double b = -acc[d][q];
+        rb[(size_t)(node * 3 + d) * K + q] = (R)b;
+        nrm2[q] += b * b;
+      }
+  }
+}
+
+// --------------------------------------------------------------- SpMM ---
+
+// Load the K values of one dof.  NC: the data is read-only for the whole
+// kernel, so the non-coherent path may be used; otherwise (vectors the same
+// kernel rewrites) plain loads keep CTA-level coherence after a barrier.
+template <typename T, int K, bool NC>
+__device__ inline void load_k(const T *p, T *o) {
+  constexpr int B = (int)sizeof(T) * K;
+  if constexpr (B % 16 == 0) {
+    const int4 *q = reinterpret_cast<const int4 *>(p);
+#pragma unroll
+    for (int x = 0; x < B / 16; x++) {
+      int4 w = NC ? __ldg(q + x) : q[x];
+      memcpy(reinterpret_cast<char *>(o) + 16 * x, &w, 16);
+    }
+  } else if constexpr (B % 8 == 0) {
+    const int2 *q = reinterpret_cast<const int2 *>(p);
+#pragma unroll
+    for (int x = 0; x < B / 8; x++) {
+      int2 w = NC ? __ldg(q + x) : q[x];
+      memcpy(reinterpret_cast<char *>(o) + 8 * x, &w, 8);
+    }
+  } else {
+#pragma unroll
+    for (int x = 0; x < K; x++) o[x] = NC ? __ldg(p + x) : p[x];
+  }
+}
+
+// y = A x for K right-hand sides, L lanes per ELL row (L divides 32), 128-bit
+// loads of values and column indices.  wp (row stride in slots) must be a
+// multiple of 4 so that every row starts on a 16-byte boundary.  Also adds sum_row x.y per load case
+// into dot[K] (lane 0 of each row group).  Every lane of a warp runs the same
+// number of loop trips, so the shuffles always see the whole warp.  NC
+// selects the non-coherent path for x (only when no thread of the kernel
+// writes x).
+template <typename T, int K, int L, bool NC = true>
+__device__ inline void spmm(int t, int nt, int nrow, int wp, const T *__restrict__ vals,
+                            const int *__restrict__ cols, const T *__restrict__ x, T *y,
+                            double *dot) {
+  constexpr int VEC = 16 / sizeof(T);    // values per 128-bit load
+  const int NCH = wp / VEC;              // 21 (FP32) or 42 (FP64) chunks per 84-slot row
+  constexpr int RPW = 32 / L;            // rows per warp per trip
+  const int lane = t & 31;
+  const int gl = lane % L;
+  const int warp = t >> 5;
+  const int nwarps = nt >> 5;
+  for (int rb = warp * RPW; rb < nrow; rb += nwarps * RPW) {
+    int row = rb + lane / L;
+    bool valid = row < nrow;
+    int rr = valid ? row : nrow - 1;
+    float acc32[K];
+    double acc64[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      acc32[q] = 0.f;
+      acc64[q] = 0.0;
+    }
+    const T *vr = vals + (size_t)rr * wp;
+    const int *cr = cols + (size_t)rr * wp;
+    for (int ch = gl; ch < NCH; ch += L) {
+      if constexpr (sizeof(T) == 4) {
+        float4 v = __ldcs(reinterpret_cast<const float4 *>(vr) + ch);
+        int4 c = __ldg(reinterpret_cast<const int4 *>(cr) + ch);
+        float vv[4] = {v.x, v.y, v.z, v.w};
+        int cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+          int col = cc[s] < 0 ? 0 : cc[s];
+          T xv[K];
+          load_k<T, K, NC>(x + (size_t)col * K, xv);
+#pragma unroll
+          for (int q = 0; q < K; q++) acc32[q] = fmaf(vv[s], xv[q], acc32[q]);
+        }
+      } else {
+        double2 v = __ldcs(reinterpret_cast<const double2 *>(vr) + ch);
+        int2 c = __ldg(reinterpret_cast<const int2 *>(cr) + ch);
+        double vv[2] = {v.x, v.y};
+        int cc[2] = {c.x, c.y};
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          int col = cc[s] < 0 ? 0 : cc[s];
+          T xv[K];
+          load_k<T, K, NC>(x + (size_t)col * K, xv);
+#pragma unroll
+          for (int q = 0; q < K; q++) acc64[q] = fma(vv[s], (double)xv[q], acc64[q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int off = L / 2; off > 0; off >>= 1)
+          acc32[q] += __shfl_xor_sync(0xffffffffu, acc32[q], off);
+      } else {
+#pragma unroll
+        for (int off = L / 2; off > 0; off >>= 1)
+          acc64[q] += __shfl_xor_sync(0xffffffffu, acc64[q], off);
+      }
+    }
+    if (valid && gl == 0) {
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        T r = (sizeof(T) == 4) ? (T)acc32[q] : (T)acc64[q];
+        y[(size_t)row * K + q] = r;
+        dot[q] += (double)r * (double)x[(size_t)row * K + q];
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------- reductions ---
+
+// Sum NV doubles over a CTA (deterministic order).  `red` is shared scratch
+// of at least 32*NV doubles; the result is broadcast to all threads in out.
+template <int NV>
+__device__ inline void block_sum(const double *v, double *red, double *out) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double w[NV];
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+    w[q] = v[q];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) w[q] += __shfl_xor_sync(0xffffffffu, w[q], off);
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; q++) red[warp * NV + q] = w[q];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      double s = (lane < nw) ? red[lane * NV + q] : 0.0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+      if (lane == 0) red[32 * NV + q] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NV; q++) out[q] = red[32 * NV + q];
+  __syncthreads();
+}
+
+// ------------------------------------------------------------ averages ---
+
+// Volume averages of strain and stress for load case q (micro/src/
+// homogenize.c:344-368): per element sum_gp w B u_e = Bbar u_e, stress =
+// D_t Bbar u_e.  Adds element sums into acc[12] (6 strain, 6 stress); the
+// caller divides by the volume.
+template <int K>
+__device__ inline void average_elems(int t, int nt, const MeshGeo &g,
+                                     const uint8_t *__restrict__ etype, const double *D /*[2][36]*/,
+                                     const double *Bbar /*[144]*/, const double *__restrict__ u,
+                                     int q, double *acc) {
+  for (int e = t; e < g.nelm; e += nt) {
+    int nod[8];
+    elem_nodes(g, e, nod);
+    double eps[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        double uv = u[(size_t)(nod[a] * 3 + d) * K + q];
+#pragma unroll
+        for (int v = 0; v < 6; v++) eps[v] = fma(Bbar[v * 24 + a * 3 + d], uv, eps[v]);
+      }
+    const double *C = D + etype[e] * 36;
+#pragma unroll
+    for (int v = 0; v < 6; v++) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < 6; w++) s = fma(C[v * 6 + w], eps[w], s);
+      acc[v] += eps[v];
+      acc[6 + v] += s;
+    }
+  }
+}
+
+}  // namespace sp

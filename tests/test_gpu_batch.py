@@ -1,0 +1,87 @@
+"""Parity of the batched persistent path (sp_batch_*): every RVE of a mixed
+batch against the oracle at the hot path's 1e-8 relative tolerance, in mixed
+(FP32 CG + FP64 refinement) and FP64 precision; results independent of the
+batch an RVE is solved in."""
+import numpy as np
+import pytest
+
+import madmax_b200 as mb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def make_descs(seed, sizes):
+    rng = np.random.default_rng(seed)
+    out = []
+    for n in sizes:
+        Em = 1e9
+        ratio = float(np.exp(rng.uniform(np.log(2), np.log(100))))
+        out.append(mb.rve_desc(int(n), float(rng.uniform(0.1, 0.35)), (Em, Em * ratio),
+                               (float(rng.uniform(0.2, 0.35)), float(rng.uniform(0.2, 0.35)))))
+    return out
+
+
+def oracle_stress(d, strains):
+    n = d.n[0]
+    m = O.cube_mesh(n)
+    et = O.fiber_types(m, [1, 1], d.radius)
+    _, st, _, _ = O.homogenize(m, et, (d.E[0], d.E[1]), (d.nu[0], d.nu[1]), strains,
+                               rtol=1e-12, lin_rtol=1e-13)
+    return st
+
+
+@pytest.mark.parametrize("precision", [mb.SP_PREC_MIXED, mb.SP_PREC_FP64])
+def test_batch_unit_tangents_match_oracle(precision):
+    sizes = [2, 3, 4, 5, 6, 8, 3, 7, 4, 6, 5, 2]
+    descs = make_descs(42, sizes)
+    b = mb.Batch(descs, precision=precision)
+    stress, strain, info = b.homogenize()
+    inf = mb.info_array(info)
+    assert (inf["status"] == 0).all(), inf
+    assert (inf["relres"] <= 1e-8).all()
+    eye = np.eye(6)
+    for i, d in enumerate(descs):
+        st = oracle_stress(d, eye)
+        assert np.abs(stress[i] - st).max() <= 1e-8 * np.abs(st).max(), i
+        assert np.allclose(strain[i], eye, atol=1e-12)
+
+
+@pytest.mark.parametrize("nrhs", [1, 4, 7, 8])
+def test_batch_custom_strains_and_materials(nrhs):
+    descs = make_descs(7, [3, 5, 4, 6])
+    rng = np.random.default_rng(nrhs)
+    strains = rng.normal(0, 1e-3, size=(len(descs), nrhs, 6))
+    mats = np.array([[2e9, 0.28, 3e10, 0.22], [1e9, 0.3, 1e9 * 50, 0.3],
+                     [5e9, 0.2, 1e10, 0.35], [1e9, 0.33, 1e11, 0.21]])
+    b = mb.Batch(descs, nrhs=nrhs)
+    stress, _, info = b.homogenize(np.ascontiguousarray(strains), mats)
+    assert (mb.info_array(info)["status"] == 0).all()
+    for i, d in enumerate(descs):
+        d.E[0], d.nu[0], d.E[1], d.nu[1] = mats[i]
+        st = oracle_stress(d, strains[i])
+        assert np.abs(stress[i] - st).max() <= 1e-8 * np.abs(st).max()
+
+
+def test_same_result_alone_and_in_mix():
+    descs = make_descs(3, [6, 2, 8, 4, 6, 3, 5, 7, 2, 4] * 3)
+    big = mb.Batch(descs)
+    s_mix, _, _ = big.homogenize()
+    for i in (0, 7, 19):
+        alone = mb.Batch([descs[i]])
+        s1, _, _ = alone.homogenize()
+        assert np.array_equal(s1[0], s_mix[i])
+    # and repeatable launch to launch
+    s_again, _, _ = big.homogenize()
+    assert np.array_equal(s_again, s_mix)
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_lane_shapes_agree(lanes):
+    descs = make_descs(9, [5, 3, 6])
+    b = mb.Batch(descs, lanes_per_row=lanes)
+    s, _, info = b.homogenize()
+    assert (mb.info_array(info)["status"] == 0).all()
+    for i, d in enumerate(descs):
+        st = oracle_stress(d, np.eye(6))
+        assert np.abs(s[i] - st).max() <= 1e-8 * np.abs(st).max()
