@@ -1,0 +1,393 @@
+"""Benchmark: RVE homogenization solves per second on B200.
+
+Workload (one "step"): 4096 independent micro-RVEs, structured hex8 meshes
+with n drawn uniformly from {8, 12, 16, 20} elements per edge, a centred
+z-aligned fiber of radius U(0.1, 0.35), matrix E = 1e9 Pa, fiber/matrix
+stiffness ratio log-uniform in [2, 100], Poisson ratios U(0.2, 0.35); each RVE
+is assembled, solved for its 6 unit-strain load cases to a 1e-8 relative FP64
+residual and volume-averaged (the 6x6 homogenized tangent).  One persistent
+launch per step, FP32 ELL values and CG with FP64 residual refinement.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank solves its own 4096 RVEs (seeded by rank, no
+collective on the data path) and rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RVE solves/sec + p50/p99 latency @1e-8 rel residual, batched-mixed vs plain GPU"
+UNIT = "RVE solves/s"
+SIZES = (8, 12, 16, 20)
+E_MATRIX = 1e9
+
+
+def workload_params(nrve: int, seed: int):
+    rng = np.random.default_rng(seed)
+    n = rng.choice(SIZES, size=nrve)
+    radius = rng.uniform(0.1, 0.35, size=nrve)
+    ratio = np.exp(rng.uniform(np.log(2.0), np.log(100.0), size=nrve))
+    nu_m = rng.uniform(0.2, 0.35, size=nrve)
+    nu_f = rng.uniform(0.2, 0.35, size=nrve)
+    return n, radius, ratio, nu_m, nu_f
+
+
+def workload_descs(mb, nrve: int, seed: int):
+    n, radius, ratio, nu_m, nu_f = workload_params(nrve, seed)
+    return [mb.rve_desc(int(n[i]), float(radius[i]), (E_MATRIX, E_MATRIX * float(ratio[i])),
+                        (float(nu_m[i]), float(nu_f[i]))) for i in range(nrve)]
+
+
+def nnz_true(n: int) -> int:
+    """Structural nonzeros of the 3D hex8 ELL matrix: 9 (3N-2)^3, N = n+1."""
+    return 9 * (3 * (n + 1) - 2) ** 3
+
+
+def algorithmic_bytes(sizes, inner_its, outer_its, k=6):
+    """Bytes the batched solve must move (FP32 values + int32 columns per
+    SpMM; FP32 CG vectors; FP64 refinement vectors; assembly writes)."""
+    total = 0.0
+    for n, it, ot in zip(sizes, inner_its, outer_its):
+        n, it, ot = int(n), float(it), float(ot)
+        ndof = 3 * (n + 1) ** 3
+        nelm = n ** 3
+        spmm = nnz_true(n) * (4 + 4) + 2 * k * ndof * 4
+        vec = 8 * k * ndof * 4
+        refine = 3 * k * ndof * 8
+        assemble = nelm * (576 * 4 + 24 * 4)
+        total += it * (spmm + vec) + (ot + 1) * refine + assemble
+    return total
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------- CPU legs ---
+
+def _oracle_rve(args):
+    n, radius, ratio, nu_m, nu_f = args
+    from oracle import oracle as O
+    m = O.cube_mesh(int(n))
+    et = O.fiber_types(m, [1.0, 1.0], float(radius))
+    t = time.perf_counter()
+    O.unit_tangent(m, et, (E_MATRIX, E_MATRIX * float(ratio)), (float(nu_m), float(nu_f)),
+                   rtol=1e-8, lin_rtol=5e-9)
+    return int(n), time.perf_counter() - t
+
+
+def cpu_sample(nrve_sample: int, seed: int, procs: int):
+    """Time the oracle (FP64 Jacobi-PCG, 6 load cases) on a sample of the
+    workload; returns seconds per RVE for each mesh size."""
+    n, radius, ratio, nu_m, nu_f = workload_params(nrve_sample, seed)
+    work = [(n[i], radius[i], ratio[i], nu_m[i], nu_f[i]) for i in range(nrve_sample)]
+    work.sort(key=lambda w: -w[0])  # largest first keeps the pool busy to the end
+    if procs > 1:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(procs) as pool:
+            pool.map(_oracle_rve, [(8, 0.2, 2.0, 0.3, 0.3)] * procs)  # start-up outside timing
+            t0 = time.perf_counter()
+            res = list(pool.imap_unordered(_oracle_rve, work, chunksize=1))
+            wall = time.perf_counter() - t0
+    else:
+        t0 = time.perf_counter()
+        res = [_oracle_rve(w) for w in work]
+        wall = time.perf_counter() - t0
+    per = {s: [t for (nn, t) in res if nn == s] for s in SIZES}
+    return per, wall, res
+
+
+def mix_rate(per_size_times):
+    """RVE/s for the uniform mix of sizes given seconds per RVE per size."""
+    mean_t = np.mean([np.mean(v) for v in per_size_times.values() if v])
+    return 1.0 / mean_t
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.lib()
+    cores = os.cpu_count() or 1
+    per_step = 4 * cores  # RVEs per step: four per core, so the pool stays busy
+    for _ in range(args.warmup):
+        cpu_sample(min(per_step, 4), 999, min(cores, 4))
+    rates = []
+    t_all = 0.0
+    for k in range(args.steps):
+        per, wall, res = cpu_sample(per_step, 2024 + k, cores)
+        rates.append(len(res) / wall)
+        t_all += wall
+    value = float(np.mean(rates))
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": "batched tangent: 4096 RVEs, n in {8,12,16,20}, 6 load cases",
+                   "sample_rves_per_step": per_step, "solver": "FP64 Jacobi-PCG (oracle port)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{per_step} seeded RVEs of the workload mix per step, "
+                                   f"spawned process pool, one process per core"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- GPU legs ---
+
+def run_ours(args):
+    import torch
+    import madmax_b200 as mb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    mb.check(mb.lib().sp_init(local), "sp_init")
+    # a real stream: events and the library's launches must share it (the
+    # legacy default stream's handle is 0, which the library reads as "its
+    # own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sptr = C.c_void_p(stream.cuda_stream)
+    assert sptr.value, "expected a non-default stream"
+
+    descs = workload_descs(mb, args.nrve, 1234 + rank)
+    sizes = [d.n[0] for d in descs]
+    t0 = time.time()
+    batch = mb.Batch(descs, nrhs=6, threads=args.threads, ctas_per_sm=args.ctas)
+    setup_s = time.time() - t0
+
+    for _ in range(args.warmup):
+        batch.launch(sptr)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timing (value) ----
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs[0].record(stream)
+    for k in range(args.steps):
+        batch.launch(sptr)
+        evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    per_launch_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    total_ms = sum(per_launch_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.nrve * args.steps / (total_ms / 1000.0)
+
+    stress = np.zeros((args.nrve, 6, 6))
+    info = (mb.sp_solve_info * args.nrve)()
+    batch.download(stress, None, info, sptr)
+    torch.cuda.synchronize()
+    inf = mb.info_array(info)
+    converged = bool((inf["status"] == 0).all())
+
+    # ---- end to end through the C ABI with host buffers ----
+    pin = lambda shape: torch.zeros(shape, dtype=torch.float64, pin_memory=True).numpy()
+    h_strain = pin((args.nrve, 6, 6))
+    for i in range(args.nrve):
+        h_strain[i] = np.eye(6)
+    h_mats = pin((args.nrve, 4))
+    for i, d in enumerate(descs):
+        h_mats[i] = (d.E[0], d.nu[0], d.E[1], d.nu[1])
+    h_stress = pin((args.nrve, 6, 6))
+    h_info = (mb.sp_solve_info * args.nrve)()
+    ee = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.e2e_steps)]
+    torch.cuda.synchronize()
+    for k in range(args.e2e_steps):
+        ee[2 * k].record(stream)
+        batch.upload(h_strain, h_mats, sptr)
+        batch.launch(sptr)
+        batch.download(h_stress, None, h_info, sptr)
+        ee[2 * k + 1].record(stream)
+        stream.synchronize()
+    e2e_ms = sum(ee[2 * k].elapsed_time(ee[2 * k + 1]) for k in range(args.e2e_steps))
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * args.nrve * args.e2e_steps / (e2e_ms / 1000.0)
+    h2d = h_strain.nbytes + h_mats.nbytes
+    d2h = h_stress.nbytes + C.sizeof(h_info)
+
+    line = None
+    if rank == 0:
+        abytes = algorithmic_bytes(sizes, inf["inner"], inf["outer"])
+        avg_ms = total_ms / args.steps
+        achieved = abytes / (avg_ms / 1000.0) / 1e9
+        peak, peak_kind = measured_peak()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": avg_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 CG + f64 refinement", "data": "synthetic",
+            "config": {"workload": f"batched tangent: {args.nrve} RVEs per GPU, n uniform in "
+                                   "{8,12,16,20}, 6 unit-strain load cases, rtol 1e-8",
+                       "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8,
+                       "precision": "mixed", "cta_threads": args.threads, "ctas_per_sm": args.ctas,
+                       "l2": "inputs larger than L2 (FP32 ELL values alone are "
+                             f"{sum(3 * (n + 1) ** 3 * 84 * 4 for n in sizes) / 1e9:.1f} GB)",
+                       "parallelism": f"replicas x{world} (independent RVEs per rank)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_kind": peak_kind, "kernel": "k_batch (persistent)"},
+            "clocks": clocks,
+            "solve": {"converged": converged, "max_relres": float(inf["relres"].max()),
+                      "mean_inner_its": float(inf["inner"].mean()),
+                      "mean_outer_its": float(inf["outer"].mean()),
+                      "rhs_solves_per_s": 6 * value, "setup_s": setup_s},
+        }
+        if world == 1 and not args.no_plain:
+            line["plain_gpu"] = plain_gpu(mb, descs, args)
+            line["plain_gpu"]["batched_speedup"] = value / line["plain_gpu"]["value"]
+        if world == 1 and not args.no_cpu:
+            per, wall, res = cpu_sample(args.cpu_sample, 77, 1)
+            line["cpu_baseline"] = {
+                "value": mix_rate(per), "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": f"{len(res)} seeded RVEs of the workload mix, FP64 Jacobi-PCG oracle "
+                          f"on 1 core ({wall:.1f} s), rate = 1 / mean over sizes of s per RVE"}
+    batch.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+def plain_gpu(mb, descs, args):
+    """The plain path: one RVE at a time, FP64 ELL + FP64 Jacobi-PCG, every
+    step a grid-wide kernel (sp_rve_tangent), on a sample of the workload."""
+    import torch
+    per = {s: [] for s in SIZES}
+    picked = []
+    for s in SIZES:
+        picked += [d for d in descs if d.n[0] == s][:args.plain_per_size]
+    for d in picked:
+        r = mb.Rve(d)
+        r.tangent()  # warm (graph build)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r.tangent()
+        per[d.n[0]].append(time.perf_counter() - t)
+        r.close()
+    return {"value": mix_rate(per), "unit": UNIT,
+            "sample": f"{len(picked)} RVEs ({args.plain_per_size} per size), FP64, one RVE "
+                      "per solve, 6 load cases per solve, host wall time per tangent",
+            "s_per_rve": {str(k): float(np.mean(v)) for k, v in per.items() if v}}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nrve", type=int, default=4096)
+    ap.add_argument("--threads", type=int, default=512)
+    ap.add_argument("--ctas", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--plain-per-size", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

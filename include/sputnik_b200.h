@@ -217,6 +217,15 @@ int sp_server_poll(sp_server *s, long long ticket, double *stress, double *tange
                    sp_solve_info *info);
 /* Stops the device loop after the queued requests finish. */
 int sp_server_stop(sp_server *s);
+/* Open-loop load generator on the calling host thread: request i (geometry
+ * geom[i], strain[i][6]) is submitted at t_arrival[i] seconds after the call
+ * starts (non-decreasing); t_done[i] receives the time its result was seen,
+ * so t_done[i] - t_arrival[i] is its latency including queueing.  Results
+ * go to stress[nreq][6], tangent[nreq][36], info[nreq] (each may be NULL).
+ * SP_ERR_TIMEOUT after timeout_s seconds. */
+int sp_server_replay(sp_server *s, int nreq, const int *geom, const double *strain,
+                     const double *t_arrival, double *t_done, double *stress, double *tangent,
+                     sp_solve_info *info, double timeout_s);
 
 #ifdef __cplusplus
 }

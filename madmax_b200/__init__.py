@@ -139,6 +139,8 @@ _PROTOS = {
     "sp_server_submit": (C.c_int, [_vp, C.c_int, _dp, C.POINTER(C.c_longlong)]),
     "sp_server_poll": (C.c_int, [_vp, C.c_longlong, _dp, _dp, C.POINTER(sp_solve_info)]),
     "sp_server_stop": (C.c_int, [_vp]),
+    "sp_server_replay": (C.c_int, [_vp, C.c_int, _ip, _dp, _dp, _dp, _dp, _dp,
+                                   C.POINTER(sp_solve_info), C.c_double]),
 }
 
 # data symbols the headers declare (fem.h tables, solvers.h selector)
@@ -386,3 +388,83 @@ def info_array(info) -> np.ndarray:
     """sp_solve_info[] -> structured numpy view (status, outer, inner, relres)."""
     return np.array([(i.status, i.outer_its, i.inner_its, i.relres) for i in info],
                     dtype=[("status", "i4"), ("outer", "i4"), ("inner", "i4"), ("relres", "f8")])
+
+
+# ------------------------------------------------------------------ serving
+
+def server_opts(**kw) -> sp_server_opts:
+    o = sp_server_opts()
+    lib().sp_server_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Server:
+    """Device-resident request loop over resident RVE geometries."""
+
+    def __init__(self, descs, **opts):
+        self.n = len(descs)
+        self.descs = (sp_rve_desc * self.n)(*descs)
+        self.opts = server_opts(**opts)
+        self.h = _vp()
+        check(lib().sp_server_create(self.n, self.descs, C.byref(self.opts), C.byref(self.h)),
+              "sp_server_create")
+
+    def start(self):
+        check(lib().sp_server_start(self.h), "sp_server_start")
+
+    def submit(self, geometry: int, strain) -> int:
+        s = np.ascontiguousarray(strain, dtype=np.float64)
+        t = C.c_longlong()
+        check(lib().sp_server_submit(self.h, geometry, ptr(s), C.byref(t)), "sp_server_submit")
+        return t.value
+
+    def poll(self, ticket: int):
+        """(stress[6], tangent[6,6], info) or None while pending."""
+        st = np.zeros(6)
+        tg = np.zeros(36)
+        info = sp_solve_info()
+        rc = lib().sp_server_poll(self.h, ticket, ptr(st), ptr(tg), C.byref(info))
+        if rc == SP_PENDING:
+            return None
+        check(rc, "sp_server_poll")
+        return st, tg.reshape(6, 6), info
+
+    def wait(self, ticket: int, timeout: float = 60.0):
+        import time
+        t0 = time.time()
+        while True:
+            r = self.poll(ticket)
+            if r is not None:
+                return r
+            if time.time() - t0 > timeout:
+                raise SputnikError(SP_ERR_TIMEOUT, f"ticket {ticket} not done after {timeout}s")
+            time.sleep(1e-4)
+
+    def replay(self, geom, strain, t_arrival, timeout=600.0):
+        n = len(geom)
+        g = np.ascontiguousarray(geom, dtype=np.int32)
+        s = np.ascontiguousarray(strain, dtype=np.float64)
+        ta = np.ascontiguousarray(t_arrival, dtype=np.float64)
+        td = np.zeros(n)
+        st = np.zeros((n, 6))
+        tg = np.zeros((n, 36))
+        info = (sp_solve_info * n)()
+        check(lib().sp_server_replay(self.h, n, ptr(g, _ip), ptr(s), ptr(ta), ptr(td), ptr(st),
+                                     ptr(tg), info, timeout), "sp_server_replay")
+        return td, st, tg.reshape(n, 6, 6), info
+
+    def stop(self):
+        check(lib().sp_server_stop(self.h), "sp_server_stop")
+
+    def close(self):
+        if self.h:
+            lib().sp_server_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -61,7 +61,9 @@ MeshGeo make_geo(const int *n, const double *len) {
   g.nx = n[0] + 1;
   g.ny = n[1] + 1;
   g.nz = n[2] + 1;
-  g.ndof = 3 * g.nx * g.ny * g.nz;
+  g.nn = g.nx * g.ny * g.nz;
+  g.nn_pad = (g.nn + 31) / 32 * 32;
+  g.ndof = 3 * g.nn;
   g.nelm = n[0] * n[1] * n[2];
   g.hx = len[0] / n[0];
   g.hy = len[1] / n[1];
@@ -71,9 +73,11 @@ MeshGeo make_geo(const int *n, const double *len) {
 }
 
 size_t plan_bytes(const int *n) {
-  size_t ndof = 3 * (size_t)(n[0] + 1) * (n[1] + 1) * (n[2] + 1);
+  size_t nn = (size_t)(n[0] + 1) * (n[1] + 1) * (n[2] + 1);
+  size_t ndof = 3 * nn, nn_pad = (nn + 31) / 32 * 32;
   size_t nelm = (size_t)n[0] * n[1] * n[2];
-  return ndof * SP_WP * sizeof(int) + nelm * SP_KE + nelm * sizeof(int);
+  return ndof * SP_WP * sizeof(int) + nelm * SP_KE + nelm * sizeof(int) +
+         nn_pad * 27 * sizeof(int);
 }
 
 static std::vector<DevPlan *> g_plans;
@@ -100,18 +104,21 @@ int plan_acquire(const int *n, DevPlan **out) {
   p->boundary_nodes = h.boundary_nodes;
   p->dev = d->id;
   size_t cb = (size_t)h.ndof * SP_WP * sizeof(int), sb = (size_t)h.nelm * SP_KE,
-         eb = (size_t)h.nelm * sizeof(int);
+         eb = (size_t)h.nelm * sizeof(int), nb = (size_t)h.nslice * 27 * 32 * sizeof(int);
   int rc = dmalloc((void **)&p->cols, cb, &p->bytes);
   if (!rc) rc = dmalloc((void **)&p->slot, sb, &p->bytes);
   if (!rc) rc = dmalloc((void **)&p->color_elems, eb, &p->bytes);
+  if (!rc) rc = dmalloc((void **)&p->nbr, nb, &p->bytes);
   if (!rc) {
     cudaError_t e1 = cudaMemcpy(p->cols, h.cols, cb, cudaMemcpyHostToDevice);
     cudaError_t e2 = cudaMemcpy(p->slot, h.slot, sb, cudaMemcpyHostToDevice);
     cudaError_t e3 = cudaMemcpy(p->color_elems, h.color_elems, eb, cudaMemcpyHostToDevice);
-    if (e1 || e2 || e3) rc = sp_set_error(SP_ERR_CUDA, "plan upload failed");
+    cudaError_t e4 = cudaMemcpy(p->nbr, h.nbr, nb, cudaMemcpyHostToDevice);
+    if (e1 || e2 || e3 || e4) rc = sp_set_error(SP_ERR_CUDA, "plan upload failed");
   }
   sp_plan_free(&h);
   if (rc) {
+    cudaFree(p->nbr);
     cudaFree(p->cols);
     cudaFree(p->slot);
     cudaFree(p->color_elems);
@@ -137,6 +144,7 @@ void plan_release(DevPlan *p) {
   int cur = -1;
   cudaGetDevice(&cur);
   cudaSetDevice(p->dev);
+  cudaFree(p->nbr);
   cudaFree(p->cols);
   cudaFree(p->slot);
   cudaFree(p->color_elems);

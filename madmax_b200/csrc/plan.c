@@ -56,6 +56,7 @@ static int neighbour_code(const sp_plan_host *p, int row_node, int col_node) {
  * the slots it hands out are the same. */
 int sp_plan_build(const int *n, sp_plan_host *p) {
   memset(p, 0, sizeof(*p));
+  p->nbr = NULL;
   if (n[0] < 1 || n[1] < 1 || n[2] < 1 || n[0] > 1024 || n[1] > 1024 || n[2] > 1024)
     return sp_set_error(SP_ERR_ARG, "mesh size %dx%dx%d out of range", n[0], n[1], n[2]);
   for (int d = 0; d < 3; d++) p->n[d] = n[d];
@@ -116,10 +117,47 @@ int sp_plan_build(const int *n, sp_plan_host *p) {
   }
   int inner = (p->nx - 2) * (p->ny - 2) * (p->nz - 2);
   p->boundary_nodes = p->nn - (inner > 0 ? inner : 0);
+  /* Node-sliced view of the same ELL rows.  Slots come in node triples:
+   * the first time an element touches (row, node b) it inserts b's three
+   * dofs in a row (the j loop of ell_add_vals runs over local dofs), and the
+   * three rows of one node receive the same columns in the same order.  So
+   * slot 3m + c of row 3a + d holds column 3 b_m(a) + c, and the 3x3 block
+   * (a, b_m) sits at slots 3m..3m+2 of rows 3a..3a+2.  nbr[s][m][l] = b_m of
+   * node a = 32 s + l; unused groups and padding nodes point at a itself
+   * (their values are zero). */
+  p->nn_pad = (p->nn + 31) / 32 * 32;
+  p->nslice = p->nn_pad / 32;
+  p->nbr = (int *)malloc((size_t)p->nslice * 27 * 32 * sizeof(int));
+  if (!p->nbr) {
+    sp_plan_free(p);
+    return sp_set_error(SP_ERR_NOMEM, "plan allocation failed");
+  }
+  for (int a = 0; a < p->nn_pad; a++) {
+    int s = a / 32, l = a % 32;
+    for (int m = 0; m < 27; m++) {
+      int b = (a < p->nn) ? a : 0;
+      if (a < p->nn) {
+        int c0 = p->cols[(size_t)(3 * a) * SP_WP + 3 * m];
+        if (c0 >= 0) {
+          b = c0 / 3;
+          /* the triple structure the slice layout relies on */
+          for (int d = 0; d < 3; d++)
+            for (int c = 0; c < 3; c++)
+              if (p->cols[(size_t)(3 * a + d) * SP_WP + 3 * m + c] != 3 * b + c) {
+                sp_plan_free(p);
+                return sp_set_error(SP_ERR_ARG, "ELL rows are not in node triples");
+              }
+        }
+      }
+      p->nbr[((size_t)s * 27 + m) * 32 + l] = b;
+    }
+  }
   return SP_OK;
 }
 
 void sp_plan_free(sp_plan_host *p) {
+  free(p->nbr);
+  p->nbr = NULL;
   free(p->cols);
   free(p->slot);
   free(p->color_elems);

@@ -30,6 +30,7 @@ namespace sp {
 struct BatchPlan {
   MeshGeo geo; // node/element counts; h and vol per RVE
   const int *cols;
+  const int *nbr;
   const uint8_t *slot;
   const int *color_elems;
   int color_off[9];
@@ -38,7 +39,7 @@ struct BatchPlan {
 struct BatchRve {
   int plan, pad;
   double len[3];
-  long long vals_off, etype_off, dinv_off;
+  long long nsv_off, etype_off, dinv_off;
 };
 
 struct BatchParams {
@@ -46,35 +47,42 @@ struct BatchParams {
   const BatchRve *rves;
   const int *order;
   int nrve, nrhs;
-  void *vals;  // float or double pool
-  void *dinv;  // float or double pool
+  void *nsv;   // float or double pool: node-sliced ELL values per RVE
+  void *dinv;  // float or double pool: component-major Jacobi diagonal per RVE
   const uint8_t *etype;
   const double *strains; // [nrve][nrhs][6]
   const double *mats;    // [nrve][4]
   double *out_stress;    // [nrve][nrhs][6]
   double *out_strain;
   sp_solve_info *out_info;
-  double *ws_u;          // per CTA [maxdof][K] FP64
-  void *ws_v;            // per CTA 4 x [maxdof][K] of T: r, x, p, q
-  size_t ws_stride;      // maxdof*K
+  double *ws_u;          // per CTA [K][3][max nn_pad] FP64
+  void *ws_v;            // per CTA 4 x [K][3][max nn_pad] of T: r, x, p, q
+  size_t ws_stride;      // K*3*max nn_pad
+  void *ws_rm;           // per CTA row-major assembly scratch [maxdof][84] of T
+  void *ws_drm;          // per CTA row-major diagonal scratch [maxdof] of T
+  size_t rm_stride;      // maxdof*84
+  size_t drm_stride;     // maxdof rounded up to 4
   int *counter;
   double rtol, inner_rtol;
   int max_outer, max_inner;
 };
 
-template <typename T, int K, int L, int NT>
-__global__ void __launch_bounds__(NT, 2) k_batch(BatchParams P) {
+template <typename T, int K, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   __shared__ double sKe[2 * SP_KE];
   __shared__ T sKeT[2 * SP_KE];
   __shared__ double sD[72], sBbar[144], sdsh[192];
   // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
   __shared__ double red[33 * 16];
   __shared__ double savg[SP_MAX_RHS * 12];
+  __shared__ CgShared sh;
   __shared__ int s_job;
   const int t = threadIdx.x;
   double *u = P.ws_u + (size_t)blockIdx.x * P.ws_stride;
   T *ws = reinterpret_cast<T *>(P.ws_v) + (size_t)blockIdx.x * 4 * P.ws_stride;
   T *r = ws, *x = ws + P.ws_stride, *p = ws + 2 * P.ws_stride, *q = ws + 3 * P.ws_stride;
+  T *vrm = reinterpret_cast<T *>(P.ws_rm) + (size_t)blockIdx.x * P.rm_stride;
+  T *drm = reinterpret_cast<T *>(P.ws_drm) + (size_t)blockIdx.x * P.drm_stride;
 
   for (;;) {
     if (t == 0) s_job = atomicAdd(P.counter, 1);
@@ -90,10 +98,9 @@ __global__ void __launch_bounds__(NT, 2) k_batch(BatchParams P) {
     g.hy = rv.len[1] / g.ney;
     g.hz = rv.len[2] / g.nez;
     g.vol = rv.len[0] * rv.len[1] * rv.len[2];
-    T *vals = reinterpret_cast<T *>(P.vals) + rv.vals_off;
+    T *nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
     T *dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
     const uint8_t *etype = P.etype + rv.etype_off;
-    const int n = g.ndof;
 
     // 1. element operators
     if (t < 2) iso_D(P.mats[rid * 4 + 2 * t], P.mats[rid * 4 + 2 * t + 1], sD + 36 * t);
@@ -103,18 +110,21 @@ __global__ void __launch_bounds__(NT, 2) k_batch(BatchParams P) {
     elem_ops_stage2(t, NT, h, sdsh, sD, 2, sKe, sBbar);
     __syncthreads();
     for (int i = t; i < 2 * SP_KE; i += NT) sKeT[i] = (T)sKe[i];
-    // 2. assembly
-    ell_zero<T>(t, NT, vals, n);
+    // 2. assembly: coloured scatter into the row-major scratch, Dirichlet
+    //    rows/columns, then the node-sliced copy the solve reads
+    ell_zero<T>(t, NT, vrm, g.ndof);
     __syncthreads();
     for (int c = 0; c < 8; c++) {
       if (pl.color_off[c + 1] > pl.color_off[c])
         scatter_colour<T>(t, NT, g, pl.color_elems, pl.color_off[c], pl.color_off[c + 1], pl.slot,
-                          etype, sKeT, vals);
+                          etype, sKeT, vrm);
       __syncthreads();
     }
-    bc_and_dinv<T>(t, NT, g, pl.cols, vals, dinv);
+    bc_and_dinv<T>(t, NT, g, pl.cols, vrm, drm);
+    __syncthreads();
+    ns_from_rows<T>(t, NT, g, pl.cols, vrm, drm, nsv, dinv);
     // load cases: u = eps . x on the boundary, 0 inside
-    affine_init<K>(t, NT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, u);
+    affine_soa<K>(t, NT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, false, u);
     __syncthreads();
 
     SolveArgs sa;
@@ -123,8 +133,8 @@ __global__ void __launch_bounds__(NT, 2) k_batch(BatchParams P) {
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
-    sp_solve_info in = solve_rve<T, K, L, NT>(g, vals, pl.cols, dinv, etype, sKe, sD, sBbar, u, r, x, p,
-                                              q, sa, red, savg);
+    sp_solve_info in = solve_rve<T, K, NT>(g, nsv, pl.nbr, dinv, etype, sKe, sD, sBbar, u, r, x, p,
+                                           q, sa, red, &sh, savg);
     if (t == 0) {
       for (int qq = 0; qq < P.nrhs; qq++) {
         size_t o = ((size_t)rid * P.nrhs + qq) * 6;
@@ -142,27 +152,22 @@ __global__ void __launch_bounds__(NT, 2) k_batch(BatchParams P) {
 // ------------------------------------------------------------- dispatch ---
 
 using BatchFn = void (*)(BatchParams);
-constexpr int BATCH_NT = 512;
 
 template <typename T, int K>
-static BatchFn pick_l(int L) {
-  switch (L) {
-    case 4: return k_batch<T, K, 4, BATCH_NT>;
-    case 16: return k_batch<T, K, 16, BATCH_NT>;
-    case 32: return k_batch<T, K, 32, BATCH_NT>;
-    default: return k_batch<T, K, 8, BATCH_NT>;
-  }
+static BatchFn pick_shape(int threads, int ctas) {
+  if (threads == 256) return ctas >= 4 ? k_batch<T, K, 256, 4> : k_batch<T, K, 256, 2>;
+  return ctas >= 2 ? k_batch<T, K, 512, 2> : k_batch<T, K, 512, 1>;
 }
 
-static BatchFn pick(int prec, int K, int L) {
+static BatchFn pick(int prec, int K, int threads, int ctas) {
   if (prec == SP_PREC_FP64) {
-    if (K == 1) return pick_l<double, 1>(L);
-    if (K <= 6) return pick_l<double, 6>(L);
-    return pick_l<double, 8>(L);
+    if (K == 1) return pick_shape<double, 1>(threads, ctas);
+    if (K <= 6) return pick_shape<double, 6>(threads, ctas);
+    return pick_shape<double, 8>(threads, ctas);
   }
-  if (K == 1) return pick_l<float, 1>(L);
-  if (K <= 6) return pick_l<float, 6>(L);
-  return pick_l<float, 8>(L);
+  if (K == 1) return pick_shape<float, 1>(threads, ctas);
+  if (K <= 6) return pick_shape<float, 6>(threads, ctas);
+  return pick_shape<float, 8>(threads, ctas);
 }
 
 static int kpad(int nrhs) { return nrhs == 1 ? 1 : (nrhs <= 6 ? 6 : 8); }
@@ -185,7 +190,7 @@ struct sp_batch_s {
   double *d_strains = nullptr, *d_mats = nullptr, *d_stress = nullptr, *d_strain = nullptr;
   sp_solve_info *d_info = nullptr;
   double *d_ws_u = nullptr;
-  void *d_ws_v = nullptr;
+  void *d_ws_v = nullptr, *d_ws_rm = nullptr, *d_ws_drm = nullptr;
   size_t bytes = 0;
 };
 
@@ -197,8 +202,8 @@ extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   o->inner_rtol = 1e-5;
   o->max_outer = 8;
   o->max_inner = 4000;
-  o->threads = BATCH_NT;
-  o->lanes_per_row = 8;
+  o->threads = 512;
+  o->lanes_per_row = 0;
   o->ctas_per_sm = 2;
 }
 
@@ -206,7 +211,7 @@ extern "C" int sp_batch_destroy(sp_batch *b) {
   if (!b) return SP_OK;
   void *bufs[] = {b->d_plans, b->d_rves, b->d_order, b->d_counter, b->d_vals, b->d_dinv,
                   b->d_etype, b->d_strains, b->d_mats, b->d_stress, b->d_strain, b->d_info,
-                  b->d_ws_u, b->d_ws_v};
+                  b->d_ws_u, b->d_ws_v, b->d_ws_rm, b->d_ws_drm};
   for (void *p : bufs) cudaFree(p);
   for (DevPlan *p : b->plans) plan_release(p);
   delete b;
@@ -225,16 +230,20 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: nrhs must be 1..%d", SP_MAX_RHS);
   if (o.precision != SP_PREC_MIXED && o.precision != SP_PREC_FP64)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown precision");
-  if (o.lanes_per_row == 0) o.lanes_per_row = 8;
-  if (o.lanes_per_row != 4 && o.lanes_per_row != 8 && o.lanes_per_row != 16 &&
-      o.lanes_per_row != 32)
-    return sp_set_error(SP_ERR_ARG, "sp_batch_create: lanes_per_row must be 4, 8, 16 or 32");
-  if (o.ctas_per_sm < 1 || o.ctas_per_sm > 2) o.ctas_per_sm = 2;
+  // CTA shape: 512 threads x 1 or 2 CTAs per SM, or 256 threads x 2 or 4
+  if (o.threads == 0) o.threads = 512;
+  if (o.threads != 256 && o.threads != 512)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: threads must be 256 or 512");
+  if (o.ctas_per_sm == 0) o.ctas_per_sm = 2;
+  if (o.threads == 512 && o.ctas_per_sm != 1 && o.ctas_per_sm != 2)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: 512-thread CTAs run 1 or 2 per SM");
+  if (o.threads == 256 && o.ctas_per_sm != 2 && o.ctas_per_sm != 4)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: 256-thread CTAs run 2 or 4 per SM");
+  o.lanes_per_row = 0;  // the node-sliced SpMM uses one lane per node (3 rows)
   if (o.max_outer < 1) o.max_outer = 8;
   if (o.max_inner < 1) o.max_inner = 4000;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
   if (!(o.inner_rtol > 0)) o.inner_rtol = 1e-5;
-  o.threads = BATCH_NT;
   for (int i = 0; i < nrve; i++)
     for (int k = 0; k < 3; k++)
       if (descs[i].n[k] < 1 || descs[i].len[k] <= 0)
@@ -255,7 +264,7 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   std::vector<BatchPlan> hplans;
   std::vector<BatchRve> hrves(nrve);
   long long voff = 0, eoff = 0, doff = 0;
-  int maxdof = 0;
+  int maxdof = 0, maxnp = 0;
   for (int i = 0; i < nrve && !rc; i++) {
     std::vector<int> key(descs[i].n, descs[i].n + 3);
     auto it = plan_index.find(key);
@@ -267,6 +276,7 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
       BatchPlan bp;
       bp.geo = p->geo;
       bp.cols = p->cols;
+      bp.nbr = p->nbr;
       bp.slot = p->slot;
       bp.color_elems = p->color_elems;
       for (int c = 0; c < 9; c++) bp.color_off[c] = p->color_off[c];
@@ -277,13 +287,14 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     BatchRve &r = hrves[i];
     r.plan = it->second;
     for (int k = 0; k < 3; k++) r.len[k] = descs[i].len[k];
-    r.vals_off = voff;
+    r.nsv_off = voff;
     r.etype_off = eoff;
     r.dinv_off = doff;
-    voff += (long long)g.ndof * SP_WP;
+    voff += (long long)g.nn_pad * 243;
     eoff += (g.nelm + 15) / 16 * 16;
-    doff += (g.ndof + 3) / 4 * 4;
+    doff += 3LL * g.nn_pad;
     maxdof = std::max(maxdof, g.ndof);
+    maxnp = std::max(maxnp, g.nn_pad);
   }
   // host-side classification into one pinned staging buffer
   uint8_t *et = nullptr;
@@ -298,7 +309,8 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   });
   int nrhs = o.nrhs, kp = b->kp;
   b->grid = d->nsm * o.ctas_per_sm;
-  size_t stride = (size_t)maxdof * kp;
+  size_t stride = (size_t)kp * 3 * maxnp;
+  size_t rm_stride = (size_t)maxdof * SP_WP, drm_stride = (size_t)(maxdof + 3) / 4 * 4;
   size_t *acct = &b->bytes;
   if (!rc) rc = dmalloc((void **)&b->d_plans, hplans.size() * sizeof(BatchPlan), acct);
   if (!rc) rc = dmalloc((void **)&b->d_rves, nrve * sizeof(BatchRve), acct);
@@ -314,6 +326,8 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (!rc) rc = dmalloc((void **)&b->d_info, (size_t)nrve * sizeof(sp_solve_info), acct);
   if (!rc) rc = dmalloc((void **)&b->d_ws_u, (size_t)b->grid * stride * sizeof(double), acct);
   if (!rc) rc = dmalloc(&b->d_ws_v, (size_t)b->grid * 4 * stride * tsz, acct);
+  if (!rc) rc = dmalloc(&b->d_ws_rm, (size_t)b->grid * rm_stride * tsz, acct);
+  if (!rc) rc = dmalloc(&b->d_ws_drm, (size_t)b->grid * drm_stride * tsz, acct);
   if (!rc) {
     // default inputs: unit strains e_0..e_{nrhs-1}, materials of the descriptors
     std::vector<double> eps((size_t)nrve * nrhs * 6, 0.0), mats((size_t)nrve * 4);
@@ -344,7 +358,7 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   P.order = b->d_order;
   P.nrve = nrve;
   P.nrhs = nrhs;
-  P.vals = b->d_vals;
+  P.nsv = b->d_vals;
   P.dinv = b->d_dinv;
   P.etype = b->d_etype;
   P.strains = b->d_strains;
@@ -355,6 +369,10 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   P.ws_u = b->d_ws_u;
   P.ws_v = b->d_ws_v;
   P.ws_stride = stride;
+  P.ws_rm = b->d_ws_rm;
+  P.ws_drm = b->d_ws_drm;
+  P.rm_stride = rm_stride;
+  P.drm_stride = drm_stride;
   P.counter = b->d_counter;
   P.rtol = o.rtol;
   P.inner_rtol = o.inner_rtol;
@@ -392,9 +410,9 @@ extern "C" int sp_batch_launch(sp_batch *b, void *stream) {
   Device *d;
   SP_TRY(device(&d));
   cudaStream_t s = pick_stream(stream, d);
-  BatchFn fn = pick(b->o.precision, b->nrhs, b->o.lanes_per_row);
+  BatchFn fn = pick(b->o.precision, b->nrhs, b->o.threads, b->o.ctas_per_sm);
   SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
-  fn<<<b->grid, BATCH_NT, 0, s>>>(b->P);
+  fn<<<b->grid, b->o.threads, 0, s>>>(b->P);
   SP_CUDA_TRY(cudaGetLastError());
   b->last_launches = 1;
   return SP_OK;

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "sp_internal.h"
 
 namespace sp {
@@ -23,6 +25,7 @@ struct MeshGeo {
   int nx, ny, nz;    // nodes per axis
   int nex, ney, nez; // elements per axis
   int ndof, nelm;
+  int nn, nn_pad;    // nodes, nodes rounded up to a multiple of 32
   double hx, hy, hz; // element edge lengths
   double vol;        // RVE volume
 };
@@ -268,25 +271,25 @@ __device__ inline void affine_boundary(int t, int nt, const MeshGeo &g, const do
 
 // Newton right-hand side b = -K u on interior dofs, 0 on boundary dofs
 // (micro/src/assembly.c:33-82 then negative_res, micro/src/homogenize.c:
-// 289-303): per node, the sum over its (up to 8) elements of Ke_t u_e.  For
-// linear elastic elements Ke_t u_e = sum_gp B^T sigma(B u_e) w exactly.
-// Writes b into rb (type R) and adds |b|^2 per load case into nrm2[K].
+// 289-303): one thread per dof row sums, over the (up to 8) elements of the
+// row's node, Ke_t[row][:] u_e.  For linear elastic elements Ke_t u_e =
+// sum_gp B^T sigma(B u_e) w exactly.  Writes b into rb (type R) and adds
+// |b|^2 per load case into nrm2[K].
 template <int K, typename R>
 __device__ inline void residual_nodes(int t, int nt, const MeshGeo &g,
                                       const uint8_t *__restrict__ etype,
                                       const double *Ke /*[2][576], shared*/,
                                       const double *__restrict__ u, R *rb, double *nrm2) {
-  int nn = g.ndof / 3;
-  for (int node = t; node < nn; node += nt) {
+  for (int row = t; row < g.ndof; row += nt) {
+    int node = row / 3, d = row % 3;
     int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
-    double acc[3][K];
+    double acc[K];
 #pragma unroll
-    for (int d = 0; d < 3; d++)
-#pragma unroll
-      for (int q = 0; q < K; q++) acc[d][q] = 0.0;
+    for (int q = 0; q < K; q++) acc[q] = 0.0;
     bool bnd = (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1);
     if (!bnd) {
       // interior node: all 8 surrounding elements exist
+#pragma unroll 1
       for (int c = 0; c < 8; c++) {
         int ox = (c & 1), oy = (c >> 1) & 1, oz = c >> 2;
         int ex = i - 1 + ox, ey = j - 1 + oy, ez = k - 1 + oz;
@@ -294,34 +297,27 @@ __device__ inline void residual_nodes(int t, int nt, const MeshGeo &g,
         // local index of this node in element e: corner (1-ox, 1-oy, 1-oz)
         int cx = 1 - ox, cy = 1 - oy, cz = 1 - oz;
         int la = cz * 4 + ((cy == 0) ? (cx ? 1 : 0) : (cx ? 2 : 3));
-        const double *ke = Ke + etype[e] * SP_KE + (la * 3) * SP_NC;
+        const double *ke = Ke + etype[e] * SP_KE + (la * 3 + d) * SP_NC;
         int n0 = ex + ey * g.nx + ez * g.nx * g.ny;
+#pragma unroll 2
         for (int b = 0; b < 8; b++) {
           int nb = n0 + corner_x(b) + corner_y(b) * g.nx + corner_z(b) * g.nx * g.ny;
           const double *ub = u + (size_t)nb * 3 * K;
 #pragma unroll
           for (int db = 0; db < 3; db++) {
-            double uv[K];
+            double kv = ke[b * 3 + db];
 #pragma unroll
-            for (int q = 0; q < K; q++) uv[q] = ub[db * K + q];
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-              double kv = ke[d * SP_NC + b * 3 + db];
-#pragma unroll
-              for (int q = 0; q < K; q++) acc[d][q] = fma(kv, uv[q], acc[d][q]);
-            }
+            for (int q = 0; q < K; q++) acc[q] = fma(kv, ub[db * K + q], acc[q]);
           }
         }
       }
     }
 #pragma unroll
-    for (int d = 0; d < 3; d++)
-#pragma unroll
-      for (int q = 0; q < K; q++) {
-        double b = -acc[d][q];
-        rb[(size_t)(node * 3 + d) * K + q] = (R)b;
-        nrm2[q] += b * b;
-      }
+    for (int q = 0; q < K; q++) {
+      double b = -acc[q];
+      rb[(size_t)row * K + q] = (R)b;
+      nrm2[q] += b * b;
+    }
   }
 }
 
@@ -432,6 +428,313 @@ __device__ inline void spmm(int t, int nt, int nrow, int wp, const T *__restrict
         y[(size_t)row * K + q] = r;
         dot[q] += (double)r * (double)x[(size_t)row * K + q];
       }
+    }
+  }
+}
+
+// y = A x on the 84-slot RVE layout with the row's value/column loads all
+// issued before its gathers (the chunk count is a compile-time constant, so
+// the loop unrolls and the loads overlap).  Same contract as spmm.
+template <typename T, int K, int L, bool NC>
+__device__ inline void spmm_rve(int t, int nt, int nrow, const T *__restrict__ vals,
+                                const int *__restrict__ cols, const T *__restrict__ x, T *y,
+                                double *dot) {
+  constexpr int VEC = 16 / sizeof(T);
+  constexpr int NCH = SP_WP / VEC;
+  constexpr int NIT = (NCH + L - 1) / L;
+  constexpr int RPW = 32 / L;
+  using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
+  const int lane = t & 31;
+  const int gl = lane % L;
+  const int warp = t >> 5;
+  const int nwarps = nt >> 5;
+  for (int rb = warp * RPW; rb < nrow; rb += nwarps * RPW) {
+    int row = rb + lane / L;
+    bool valid = row < nrow;
+    int rr = valid ? row : nrow - 1;
+    const int4 *vr = reinterpret_cast<const int4 *>(vals + (size_t)rr * SP_WP);
+    const int *cr = cols + (size_t)rr * SP_WP;
+    int4 vv[NIT];
+    int cc[NIT][VEC];
+#pragma unroll
+    for (int it = 0; it < NIT; it++) {
+      int ch = gl + it * L;
+      if (ch < NCH) {
+        vv[it] = __ldcs(vr + ch);
+        if constexpr (VEC == 4) {
+          int4 c = __ldg(reinterpret_cast<const int4 *>(cr) + ch);
+          cc[it][0] = c.x; cc[it][1] = c.y; cc[it][2] = c.z; cc[it][3] = c.w;
+        } else {
+          int2 c = __ldg(reinterpret_cast<const int2 *>(cr) + ch);
+          cc[it][0] = c.x; cc[it][1] = c.y;
+        }
+      } else {
+        vv[it] = make_int4(0, 0, 0, 0);
+#pragma unroll
+        for (int s = 0; s < VEC; s++) cc[it][s] = -1;
+      }
+    }
+    A acc[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) acc[q] = A(0);
+#pragma unroll
+    for (int it = 0; it < NIT; it++) {
+      T v[VEC];
+      memcpy(v, &vv[it], 16);
+#pragma unroll
+      for (int s = 0; s < VEC; s++) {
+        int col = cc[it][s] < 0 ? 0 : cc[it][s];
+        T xv[K];
+        load_k<T, K, NC>(x + (size_t)col * K, xv);
+#pragma unroll
+        for (int q = 0; q < K; q++) acc[q] = fma((A)v[s], (A)xv[q], acc[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++)
+#pragma unroll
+      for (int off = L / 2; off > 0; off >>= 1)
+        acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    if (valid && gl == 0) {
+      T o[K];
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        o[q] = (T)acc[q];
+        dot[q] += (double)o[q] * (double)x[(size_t)row * K + q];
+      }
+#pragma unroll
+      for (int q = 0; q < K; q++) y[(size_t)row * K + q] = o[q];
+    }
+  }
+}
+
+// Row-chunked access to [rows][K] vectors with 16-byte loads: a super-chunk
+// holds S = lcm(K, 16/sizeof(T)) values = RPC whole rows, so the load case of
+// every element is a compile-time constant.  Vectors are padded to a
+// multiple of 4 rows (zero-filled), which every RPC divides.
+template <typename T, int K>
+struct Chunks {
+  static constexpr int E = 16 / sizeof(T);
+  static constexpr int gcd(int a, int b) { return b ? gcd(b, a % b) : a; }
+  static constexpr int S = K / gcd(K, E) * E;
+  static constexpr int RPC = S / K;
+  static constexpr int NV = S / E;
+  __device__ static void load(const T *p, T *v) {
+    const int4 *q = reinterpret_cast<const int4 *>(p);
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      int4 w = q[i];
+      memcpy(reinterpret_cast<char *>(v) + 16 * i, &w, 16);
+    }
+  }
+  __device__ static void store(T *p, const T *v) {
+    int4 *q = reinterpret_cast<int4 *>(p);
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      int4 w;
+      memcpy(&w, reinterpret_cast<const char *>(v) + 16 * i, 16);
+      q[i] = w;
+    }
+  }
+};
+
+// ------------------------------------------------ node-sliced ELL path ---
+//
+// The batched and serving solves read each RVE's ELL matrix through a
+// node-sliced copy of the same values: the 3x3 block (node a, group m) of
+// rows 3a..3a+2, slots 3m..3m+2 is stored at
+//   nsv[((s*27 + m)*9 + 3d + c)*32 + l],  a = 32 s + l,
+// with the block's column node in nbr[(s*27 + m)*32 + l].  A warp owns a
+// slice of 32 consecutive nodes, a lane one node (three rows).  Values,
+// neighbour ids and the K-vectors of neighbours are then all read with
+// whole-warp coalesced accesses (interior nodes of a slice share the group
+// order, so their neighbours are consecutive too).  Vectors are
+// component-major: v[(k*3 + d)*nn_pad + node].
+
+// Row-major ELL (values after Dirichlet) -> node-sliced values and the
+// component-major Jacobi diagonal.
+template <typename T>
+__device__ inline void ns_from_rows(int t, int nt, const MeshGeo &g, const int *__restrict__ cols,
+                                    const T *vals_rm, const T *dinv_rm, T *nsv, T *dinv) {
+  const size_t total = (size_t)(g.nn_pad / 32) * 27 * 9 * 32;
+  for (size_t x = t; x < total; x += nt) {
+    int l = (int)(x % 32);
+    size_t q = x / 32;
+    int i = (int)(q % 9);
+    size_t sm = q / 9;
+    int m = (int)(sm % 27), s = (int)(sm / 27);
+    int a = s * 32 + l, d = i / 3, c = i % 3;
+    T v = T(0);
+    if (a < g.nn) {
+      size_t o = (size_t)(3 * a + d) * SP_WP + 3 * m + c;
+      if (cols[o] >= 0) v = vals_rm[o];
+    }
+    nsv[x] = v;
+  }
+  for (int x = t; x < 3 * g.nn_pad; x += nt) {
+    int d = x / g.nn_pad, a = x % g.nn_pad;
+    dinv[x] = (a < g.nn) ? dinv_rm[3 * a + d] : T(0);
+  }
+}
+
+// y = A x (K right-hand sides) on the node-sliced layout; adds x.y per load
+// case into dot[K].
+template <typename T, int K, bool NC>
+__device__ inline void spmm_ns(int t, int nt, const MeshGeo &g, const T *__restrict__ nsv,
+                               const int *__restrict__ nbr, const T *__restrict__ x, T *y,
+                               double *dot) {
+  using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
+  const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
+  const int nslice = g.nn_pad / 32;
+  const size_t blk = (size_t)3 * g.nn_pad;
+  for (int s = warp; s < nslice; s += nwarps) {
+    A acc[3][K];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int k = 0; k < K; k++) acc[d][k] = A(0);
+    const T *vs = nsv + (size_t)s * 27 * 9 * 32 + lane;
+    const int *bs = nbr + (size_t)s * 27 * 32 + lane;
+#pragma unroll 3
+    for (int m = 0; m < 27; m++) {
+      int b = __ldg(bs + m * 32);
+      T v[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) v[i] = __ldcs(vs + (m * 9 + i) * 32);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        A xb[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const T *xp = x + k * blk + (size_t)c * g.nn_pad + b;
+          xb[c] = NC ? (A)__ldg(xp) : (A)*xp;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) acc[d][k] = fma((A)v[d * 3 + c], xb[c], acc[d][k]);
+      }
+    }
+    const int a = s * 32 + lane;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        size_t o = k * blk + (size_t)d * g.nn_pad + a;
+        T yv = (T)acc[d][k];
+        dot[k] += (double)yv * (double)x[o];
+        y[o] = yv;
+      }
+  }
+}
+
+// b = -K u on interior dofs, 0 on the boundary and on padding (component-
+// major vectors; see residual_nodes for the arithmetic).
+template <int K, typename R>
+__device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
+                                    const uint8_t *__restrict__ etype,
+                                    const double *Ke /*[2][576], shared*/,
+                                    const double *__restrict__ u, R *rb, double *nrm2) {
+  const size_t blk = (size_t)3 * g.nn_pad;
+  for (int idx = t; idx < 3 * g.nn_pad; idx += nt) {
+    int d = idx / g.nn_pad, node = idx % g.nn_pad;
+    double acc[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) acc[q] = 0.0;
+    if (node < g.nn) {
+      int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+      bool bnd = (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1);
+      if (!bnd) {
+#pragma unroll 1
+        for (int c = 0; c < 8; c++) {
+          int ox = (c & 1), oy = (c >> 1) & 1, oz = c >> 2;
+          int ex = i - 1 + ox, ey = j - 1 + oy, ez = k - 1 + oz;
+          int e = ex + ey * g.nex + ez * g.nex * g.ney;
+          int cx = 1 - ox, cy = 1 - oy, cz = 1 - oz;
+          int la = cz * 4 + ((cy == 0) ? (cx ? 1 : 0) : (cx ? 2 : 3));
+          const double *ke = Ke + etype[e] * SP_KE + (la * 3 + d) * SP_NC;
+          int n0 = ex + ey * g.nx + ez * g.nx * g.ny;
+#pragma unroll 2
+          for (int b = 0; b < 8; b++) {
+            int nb = n0 + corner_x(b) + corner_y(b) * g.nx + corner_z(b) * g.nx * g.ny;
+#pragma unroll
+            for (int db = 0; db < 3; db++) {
+              double kv = ke[b * 3 + db];
+#pragma unroll
+              for (int q = 0; q < K; q++)
+                acc[q] = fma(kv, u[q * blk + (size_t)db * g.nn_pad + nb], acc[q]);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      double b = -acc[q];
+      rb[q * blk + idx] = (R)b;
+      nrm2[q] += b * b;
+    }
+  }
+}
+
+// u = eps . x on boundary dofs; interior dofs are set to 0 (keep_inside =
+// false) or kept (warm start); load cases >= nrhs and padding are 0.
+template <int K>
+__device__ inline void affine_soa(int t, int nt, const MeshGeo &g, const double *eps, int nrhs,
+                                  bool keep_inside, double *u) {
+  const size_t blk = (size_t)3 * g.nn_pad;
+  for (size_t x = t; x < K * blk; x += nt) {
+    int k = (int)(x / blk);
+    int rem = (int)(x % blk);
+    int d = rem / g.nn_pad, node = rem % g.nn_pad;
+    if (node >= g.nn || k >= nrhs) {
+      u[x] = 0.0;
+      continue;
+    }
+    if (!is_bnode(g, node)) {
+      if (!keep_inside) u[x] = 0.0;
+      continue;
+    }
+    int i = node % g.nx, j = (node / g.nx) % g.ny, kk = node / (g.nx * g.ny);
+    double X = i * g.hx, Y = j * g.hy, Z = kk * g.hz;
+    const double *e = eps + k * 6;
+    double val;
+    if (d == 0)
+      val = dadd(dadd(dmul(e[0], X), dmul(e[3] / 2, Y)), dmul(e[5] / 2, Z));
+    else if (d == 1)
+      val = dadd(dadd(dmul(e[3] / 2, X), dmul(e[1], Y)), dmul(e[4] / 2, Z));
+    else
+      val = dadd(dadd(dmul(e[5] / 2, X), dmul(e[4] / 2, Y)), dmul(e[2], Z));
+    u[x] = val;
+  }
+}
+
+// volume averages of load case q on component-major u (see average_elems)
+__device__ inline void average_soa(int t, int nt, const MeshGeo &g,
+                                   const uint8_t *__restrict__ etype, const double *D,
+                                   const double *Bbar, const double *__restrict__ u, int q,
+                                   double *acc) {
+  const size_t blk = (size_t)3 * g.nn_pad;
+  for (int e = t; e < g.nelm; e += nt) {
+    int nod[8];
+    elem_nodes(g, e, nod);
+    double eps[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        double uv = u[q * blk + (size_t)d * g.nn_pad + nod[a]];
+#pragma unroll
+        for (int v = 0; v < 6; v++) eps[v] = fma(Bbar[v * 24 + a * 3 + d], uv, eps[v]);
+      }
+    const double *C = D + etype[e] * 36;
+#pragma unroll
+    for (int v = 0; v < 6; v++) {
+      double s = 0.0;
+#pragma unroll
+      for (int w = 0; w < 6; w++) s = fma(C[v * 6 + w], eps[w], s);
+      acc[v] += eps[v];
+      acc[6 + v] += s;
     }
   }
 }

@@ -44,6 +44,7 @@ struct DevPlan {
   MeshGeo geo;             // h and vol filled per RVE, not here
   int color_off[9];
   int *cols = nullptr;     // [ndof][SP_WP]
+  int *nbr = nullptr;      // [nslice][27][32] node-sliced neighbour ids
   uint8_t *slot = nullptr; // [nelm][576]
   int *color_elems = nullptr;
   int boundary_nodes = 0;

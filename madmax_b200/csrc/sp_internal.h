@@ -30,7 +30,9 @@ typedef struct {
   int nn, ndof, nelm;
   int boundary_nodes;
   int color_off[9];    /* elements of colour c: color_elems[color_off[c] .. color_off[c+1]) */
+  int nn_pad, nslice;  /* nodes rounded up to 32, slices of 32 nodes */
   int *cols;           /* host [ndof][SP_WP], first-touch order, -1 padded */
+  int *nbr;            /* host [nslice][27][32]: neighbour node of group m (see plan.c) */
   uint8_t *slot;       /* host [nelm][576]: slot (within the row) of Ke entry (i, j) */
   int *color_elems;    /* host [nelm] */
 } sp_plan_host;

@@ -76,10 +76,10 @@ def test_same_result_alone_and_in_mix():
     assert np.array_equal(s_again, s_mix)
 
 
-@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
-def test_lane_shapes_agree(lanes):
+@pytest.mark.parametrize("threads,ctas", [(512, 1), (512, 2), (256, 2), (256, 4)])
+def test_cta_shapes_agree(threads, ctas):
     descs = make_descs(9, [5, 3, 6])
-    b = mb.Batch(descs, lanes_per_row=lanes)
+    b = mb.Batch(descs, threads=threads, ctas_per_sm=ctas)
     s, _, info = b.homogenize()
     assert (mb.info_array(info)["status"] == 0).all()
     for i, d in enumerate(descs):

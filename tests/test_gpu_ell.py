@@ -109,3 +109,23 @@ def test_ell_dev_mvp_and_pcg():
         assert np.abs(xg - xo).max() <= 1e-8 * np.abs(xo).max()
     finally:
         mb.lib().sp_ell_dev_free(h)
+
+
+def test_reference_unity_program_linked_to_library(golden_dir, tmp_path):
+    """The reference's unity/unity_ell.c, compiled unchanged against
+    include/ell.h and linked to libsputnik_b200.so (oracle/Makefile target
+    dropin), prints what the reference build prints."""
+    import subprocess
+    exe = os.path.join(os.path.dirname(O.LIB_PATH), "_ref", "unity_ell_b200")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in build of unity_ell.c not present")
+    out = subprocess.run([exe], cwd=tmp_path, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    d = json.load(open(os.path.join(golden_dir, "unity_ell.json")))
+    lines = out.stdout.splitlines()
+    i0 = lines.index("m=")
+    mat = [[float(v) for v in ln.split()] for ln in lines[i0 + 1:i0 + 11]]
+    assert mat == d["printed_matrix"]
+    assert int([ln for ln in lines if ln.startswith("its")][0].split("=")[1]) == 388
+    x = [float(v) for v in open(tmp_path / "sol.dat").read().split()]
+    assert x == d["printed_x"]

@@ -1,0 +1,107 @@
+"""The device-resident serving loop (sp_server_*): results against the
+oracle's finite-difference tangent (micro/src/homogenize.c:59-94), the same
+request alone and in a mix of concurrent requests, the replay driver, and
+admission by HBM budget."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import madmax_b200 as mb
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def geoms():
+    rng = np.random.default_rng(17)
+    out = []
+    for n in (3, 4, 5, 6, 4, 8):
+        ratio = float(np.exp(rng.uniform(np.log(2), np.log(100))))
+        out.append(mb.rve_desc(n, float(rng.uniform(0.1, 0.35)), (1e9, 1e9 * ratio),
+                               (float(rng.uniform(0.2, 0.35)), float(rng.uniform(0.2, 0.35)))))
+    return out
+
+
+def oracle_fd(d, eps):
+    m = O.cube_mesh(d.n[0])
+    et = O.fiber_types(m, [1, 1], d.radius)
+    Cm, s0 = O.fd_tangent(m, et, (d.E[0], d.E[1]), (d.nu[0], d.nu[1]), eps, rtol=1e-12,
+                          lin_rtol=1e-13)
+    return s0, Cm
+
+
+def test_serve_matches_oracle():
+    G = geoms()
+    s = mb.Server(G)
+    s.start()
+    rng = np.random.default_rng(1)
+    reqs = [(int(rng.integers(0, len(G))), rng.normal(0, 1e-3, 6)) for _ in range(12)]
+    tickets = [s.submit(g, e) for g, e in reqs]
+    for tk, (g, e) in zip(tickets, reqs):
+        st, tg, info = s.wait(tk)
+        assert info.status == 0 and info.relres <= 1e-8
+        s0, Cm = oracle_fd(G[g], e)
+        assert np.abs(st - s0).max() <= 1e-8 * np.abs(s0).max()
+        assert np.abs(tg - Cm).max() <= 1e-7 * np.abs(Cm).max()
+    s.stop()
+    s.close()
+
+
+def test_same_result_alone_and_in_mix():
+    G = geoms()
+    e = np.array([1e-3, -5e-4, 2e-4, 3e-4, 0.0, -1e-4])
+    a = mb.Server(G)
+    a.start()
+    st_alone, tg_alone, _ = a.wait(a.submit(3, e))
+    a.stop()
+    a.close()
+    b = mb.Server(G)
+    b.start()
+    rng = np.random.default_rng(2)
+    burst = [b.submit(int(rng.integers(0, len(G))), rng.normal(0, 1e-3, 6)) for _ in range(20)]
+    mine = b.submit(3, e)
+    burst += [b.submit(int(rng.integers(0, len(G))), rng.normal(0, 1e-3, 6)) for _ in range(20)]
+    st_mix, tg_mix, info = b.wait(mine)
+    for tk in burst:
+        assert b.wait(tk)[2].status == 0
+    b.stop()
+    b.close()
+    # warm starts differ between the two runs: equal within the solve tolerance
+    assert np.abs(st_mix - st_alone).max() <= 2e-8 * np.abs(st_alone).max()
+    assert np.abs(tg_mix - tg_alone).max() <= 2e-7 * np.abs(tg_alone).max()
+
+
+def test_replay_poisson_latencies():
+    G = geoms()
+    s = mb.Server(G)
+    rng = np.random.default_rng(3)
+    n = 200
+    t_arr = np.cumsum(rng.exponential(1.0 / 2000.0, size=n))
+    geo = rng.integers(0, len(G), size=n)
+    eps = rng.normal(0, 1e-3, size=(n, 6))
+    td, st, tg, info = s.replay(geo, eps, t_arr, timeout=120)
+    lat = td - t_arr
+    assert (lat > 0).all()
+    assert all(i.status == 0 for i in info)
+    # spot-check a few against the oracle
+    for i in (0, 57, 199):
+        s0, Cm = oracle_fd(G[geo[i]], eps[i])
+        assert np.abs(st[i] - s0).max() <= 1e-8 * np.abs(s0).max()
+    s.stop()
+    s.close()
+
+
+def test_budget_refusal_and_bad_geometry():
+    G = geoms()
+    descs = (mb.sp_rve_desc * len(G))(*G)
+    o = mb.server_opts(hbm_budget=1 << 20)
+    h = mb._vp()
+    assert mb.lib().sp_server_create(len(G), descs, C.byref(o), C.byref(h)) == mb.SP_ERR_BUDGET
+    s = mb.Server(G)
+    s.start()
+    t = C.c_longlong()
+    e = np.zeros(6)
+    assert mb.lib().sp_server_submit(s.h, len(G), mb.ptr(e), C.byref(t)) == mb.SP_ERR_RANGE
+    s.stop()
+    s.close()
