@@ -59,14 +59,17 @@ def nnz_true(n: int) -> int:
 
 
 def algorithmic_bytes(sizes, inner_its, outer_its, k=6):
-    """Bytes the batched solve must move (FP32 values + int32 columns per
-    SpMM; FP32 CG vectors; FP64 refinement vectors; assembly writes)."""
+    """Bytes the batched solve must move per launch: per CG iteration the
+    FP32 matrix values (4 B per structural nonzero) plus one int32 column
+    node per 3x3 block (the node-sliced ELL stores one per block), the SpMM
+    input/output vectors and 8 FP32 vector passes; per refinement step 3 FP64
+    vector passes; the assembly writes once."""
     total = 0.0
     for n, it, ot in zip(sizes, inner_its, outer_its):
         n, it, ot = int(n), float(it), float(ot)
         ndof = 3 * (n + 1) ** 3
         nelm = n ** 3
-        spmm = nnz_true(n) * (4 + 4) + 2 * k * ndof * 4
+        spmm = nnz_true(n) * 4 + nnz_true(n) // 9 * 4 + 2 * k * ndof * 4
         vec = 8 * k * ndof * 4
         refine = 3 * k * ndof * 8
         assemble = nelm * (576 * 4 + 24 * 4)
@@ -233,7 +236,8 @@ def run_ours(args):
     descs = workload_descs(mb, args.nrve, 1234 + rank)
     sizes = [d.n[0] for d in descs]
     t0 = time.time()
-    batch = mb.Batch(descs, nrhs=6, threads=args.threads, ctas_per_sm=args.ctas)
+    batch = mb.Batch(descs, nrhs=6, threads=args.threads, ctas_per_sm=args.ctas,
+                     cluster=args.cluster)
     setup_s = time.time() - t0
 
     for _ in range(args.warmup):
@@ -314,6 +318,7 @@ def run_ours(args):
                                    "{8,12,16,20}, 6 unit-strain load cases, rtol 1e-8",
                        "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8,
                        "precision": "mixed", "cta_threads": args.threads, "ctas_per_sm": args.ctas,
+                       "cluster": args.cluster,
                        "l2": "inputs larger than L2 (FP32 ELL values alone are "
                              f"{sum(3 * (n + 1) ** 3 * 84 * 4 for n in sizes) / 1e9:.1f} GB)",
                        "parallelism": f"replicas x{world} (independent RVEs per rank)"},
@@ -332,6 +337,8 @@ def run_ours(args):
         if world == 1 and not args.no_plain:
             line["plain_gpu"] = plain_gpu(mb, descs, args)
             line["plain_gpu"]["batched_speedup"] = value / line["plain_gpu"]["value"]
+        if world == 1 and not args.no_serve:
+            line["serving"] = serving(mb, args)
         if world == 1 and not args.no_cpu:
             per, wall, res = cpu_sample(args.cpu_sample, 77, 1)
             line["cpu_baseline"] = {
@@ -344,6 +351,84 @@ def run_ours(args):
         dist.destroy_process_group()
     if line:
         print(json.dumps(line), flush=True)
+
+
+def serve_geometries(mb, ngeom: int, seed: int):
+    """256 resident geometries, n uniform in 8..32, fibers and materials as
+    in the batched workload."""
+    rng = np.random.default_rng(seed)
+    n = rng.integers(8, 33, size=ngeom)
+    radius = rng.uniform(0.1, 0.35, size=ngeom)
+    ratio = np.exp(rng.uniform(np.log(2.0), np.log(100.0), size=ngeom))
+    nu_m = rng.uniform(0.2, 0.35, size=ngeom)
+    nu_f = rng.uniform(0.2, 0.35, size=ngeom)
+    return [mb.rve_desc(int(n[i]), float(radius[i]), (E_MATRIX, E_MATRIX * float(ratio[i])),
+                        (float(nu_m[i]), float(nu_f[i]))) for i in range(ngeom)]
+
+
+def serving(mb, args):
+    """Open-loop Poisson load on the device-resident server; the plain path
+    is one FIFO server whose service times are measured per geometry with
+    the plain FP64 solve of the same 7 load cases."""
+    import torch
+    geoms = serve_geometries(mb, args.serve_geoms, 4321)
+    t0 = time.time()
+    srv = mb.Server(geoms, hbm_budget=150 * 10 ** 9)
+    setup = time.time() - t0
+    srv.start()
+    rng = np.random.default_rng(99)
+    # warm every geometry once (first solves start from zero)
+    warm_g = np.arange(len(geoms))
+    srv.replay(warm_g, rng.normal(0, 1e-3, (len(geoms), 6)), np.zeros(len(geoms)), timeout=600)
+    out = {"geometries": len(geoms), "n_range": [8, 32], "setup_s": setup, "rates": {}}
+    plain_samples = {}
+    for lam in args.serve_rates:
+        nreq = int(min(args.serve_max_req, max(200, lam * args.serve_seconds)))
+        t_arr = np.cumsum(rng.exponential(1.0 / lam, size=nreq))
+        geo = rng.integers(0, len(geoms), size=nreq)
+        eps = rng.normal(0, 1e-3, size=(nreq, 6))
+        td, st, tg, info = srv.replay(geo, eps, t_arr, timeout=900)
+        lat = (td - t_arr) * 1000.0
+        ok = all(i.status == 0 for i in info)
+        span = td.max() - t_arr.min()
+        out["rates"][str(lam)] = {"requests": nreq, "p50_ms": float(np.percentile(lat, 50)),
+                                  "p99_ms": float(np.percentile(lat, 99)),
+                                  "solves_per_s": nreq / span, "all_converged": ok}
+        plain_samples[lam] = (t_arr, geo)
+    srv.stop()
+    srv.close()
+    # plain: service time per geometry (7 load cases, FP64, one RVE at a time)
+    sizes = sorted(set(int(g.n[0]) for g in geoms))
+    probe = [s for s in sizes if s in (8, 14, 20, 26, 32)] or sizes[:3]
+    svc = {}
+    for sz in probe:
+        d = next(g for g in geoms if g.n[0] == sz)
+        r = mb.Rve(d)
+        e = np.tile(rng.normal(0, 1e-3, 6), (7, 1))
+        for i in range(6):
+            e[i + 1, i] += 0.005
+        r.homogenize(e)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r.homogenize(e)
+        svc[sz] = time.perf_counter() - t
+        r.close()
+    xs = np.array(sorted(svc))
+    ys = np.array([svc[k] for k in xs])
+    for lam, (t_arr, geo) in plain_samples.items():
+        service = np.interp([geoms[g].n[0] for g in geo], xs, ys)
+        free = 0.0
+        lat = np.zeros(len(t_arr))
+        for i, (ta, sv) in enumerate(zip(t_arr, service)):
+            start = max(ta, free)
+            free = start + sv
+            lat[i] = (free - ta) * 1000.0
+        span = free - t_arr.min()
+        out["rates"][str(lam)]["plain"] = {"p50_ms": float(np.percentile(lat, 50)),
+                                           "p99_ms": float(np.percentile(lat, 99)),
+                                           "solves_per_s": len(t_arr) / span}
+    out["plain_service_s"] = {str(k): float(v) for k, v in svc.items()}
+    return out
 
 
 def plain_gpu(mb, descs, args):
@@ -377,11 +462,17 @@ def main(argv=None):
     ap.add_argument("--nrve", type=int, default=4096)
     ap.add_argument("--threads", type=int, default=512)
     ap.add_argument("--ctas", type=int, default=2)
+    ap.add_argument("--cluster", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--plain-per-size", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-geoms", type=int, default=256)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[1e3, 1e4, 1e5])
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-max-req", type=int, default=4000)
     args = ap.parse_args(argv)
     if args.impl == "reference":
         run_reference(args)

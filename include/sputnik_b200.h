@@ -146,8 +146,8 @@ typedef struct {
   int max_inner;     /* CG iterations per step (default 4000) */
   int threads;       /* threads per CTA (0: tuned) */
   int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
-  int ctas_per_sm;   /* resident CTAs per SM (0: tuned) */
-  int pad;
+  int ctas_per_sm;   /* resident CTAs per SM: 1 or 2 (512 threads), 2 or 4 (256) */
+  int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 */
 } sp_batch_opts;
 
 void sp_batch_opts_default(sp_batch_opts *o);

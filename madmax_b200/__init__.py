@@ -63,7 +63,7 @@ class sp_batch_opts(C.Structure):
     _fields_ = [("nrhs", C.c_int), ("precision", C.c_int), ("rtol", C.c_double),
                 ("inner_rtol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
                 ("threads", C.c_int), ("lanes_per_row", C.c_int), ("ctas_per_sm", C.c_int),
-                ("pad", C.c_int)]
+                ("cluster", C.c_int)]
 
 
 class sp_server_opts(C.Structure):

@@ -22,152 +22,45 @@
 #include <map>
 #include <vector>
 
-#include "rve_solve.cuh"
-#include "sp_cuda.h"
+#include "rve_batch_kernel.cuh"
 
 namespace sp {
 
-struct BatchPlan {
-  MeshGeo geo; // node/element counts; h and vol per RVE
-  const int *cols;
-  const int *nbr;
-  const uint8_t *slot;
-  const int *color_elems;
-  int color_off[9];
-};
-
-struct BatchRve {
-  int plan, pad;
-  double len[3];
-  long long nsv_off, etype_off, dinv_off;
-};
-
-struct BatchParams {
-  const BatchPlan *plans;
-  const BatchRve *rves;
-  const int *order;
-  int nrve, nrhs;
-  void *nsv;   // float or double pool: node-sliced ELL values per RVE
-  void *dinv;  // float or double pool: component-major Jacobi diagonal per RVE
-  const uint8_t *etype;
-  const double *strains; // [nrve][nrhs][6]
-  const double *mats;    // [nrve][4]
-  double *out_stress;    // [nrve][nrhs][6]
-  double *out_strain;
-  sp_solve_info *out_info;
-  double *ws_u;          // per CTA [K][3][max nn_pad] FP64
-  void *ws_v;            // per CTA 4 x [K][3][max nn_pad] of T: r, x, p, q
-  size_t ws_stride;      // K*3*max nn_pad
-  void *ws_rm;           // per CTA row-major assembly scratch [maxdof][84] of T
-  void *ws_drm;          // per CTA row-major diagonal scratch [maxdof] of T
-  size_t rm_stride;      // maxdof*84
-  size_t drm_stride;     // maxdof rounded up to 4
-  int *counter;
-  double rtol, inner_rtol;
-  int max_outer, max_inner;
-};
-
-template <typename T, int K, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
-  __shared__ double sKe[2 * SP_KE];
-  __shared__ T sKeT[2 * SP_KE];
-  __shared__ double sD[72], sBbar[144], sdsh[192];
-  // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
-  __shared__ double red[33 * 16];
-  __shared__ double savg[SP_MAX_RHS * 12];
-  __shared__ CgShared sh;
-  __shared__ int s_job;
-  const int t = threadIdx.x;
-  double *u = P.ws_u + (size_t)blockIdx.x * P.ws_stride;
-  T *ws = reinterpret_cast<T *>(P.ws_v) + (size_t)blockIdx.x * 4 * P.ws_stride;
-  T *r = ws, *x = ws + P.ws_stride, *p = ws + 2 * P.ws_stride, *q = ws + 3 * P.ws_stride;
-  T *vrm = reinterpret_cast<T *>(P.ws_rm) + (size_t)blockIdx.x * P.rm_stride;
-  T *drm = reinterpret_cast<T *>(P.ws_drm) + (size_t)blockIdx.x * P.drm_stride;
-
-  for (;;) {
-    if (t == 0) s_job = atomicAdd(P.counter, 1);
-    __syncthreads();
-    int job = s_job;
-    __syncthreads();
-    if (job >= P.nrve) break;
-    const int rid = P.order[job];
-    const BatchRve rv = P.rves[rid];
-    const BatchPlan pl = P.plans[rv.plan];
-    MeshGeo g = pl.geo;
-    g.hx = rv.len[0] / g.nex;
-    g.hy = rv.len[1] / g.ney;
-    g.hz = rv.len[2] / g.nez;
-    g.vol = rv.len[0] * rv.len[1] * rv.len[2];
-    T *nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
-    T *dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
-    const uint8_t *etype = P.etype + rv.etype_off;
-
-    // 1. element operators
-    if (t < 2) iso_D(P.mats[rid * 4 + 2 * t], P.mats[rid * 4 + 2 * t + 1], sD + 36 * t);
-    double h[3] = {g.hx, g.hy, g.hz};
-    elem_ops_stage1(t, NT, h, sdsh);
-    __syncthreads();
-    elem_ops_stage2(t, NT, h, sdsh, sD, 2, sKe, sBbar);
-    __syncthreads();
-    for (int i = t; i < 2 * SP_KE; i += NT) sKeT[i] = (T)sKe[i];
-    // 2. assembly: coloured scatter into the row-major scratch, Dirichlet
-    //    rows/columns, then the node-sliced copy the solve reads
-    ell_zero<T>(t, NT, vrm, g.ndof);
-    __syncthreads();
-    for (int c = 0; c < 8; c++) {
-      if (pl.color_off[c + 1] > pl.color_off[c])
-        scatter_colour<T>(t, NT, g, pl.color_elems, pl.color_off[c], pl.color_off[c + 1], pl.slot,
-                          etype, sKeT, vrm);
-      __syncthreads();
-    }
-    bc_and_dinv<T>(t, NT, g, pl.cols, vrm, drm);
-    __syncthreads();
-    ns_from_rows<T>(t, NT, g, pl.cols, vrm, drm, nsv, dinv);
-    // load cases: u = eps . x on the boundary, 0 inside
-    affine_soa<K>(t, NT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, false, u);
-    __syncthreads();
-
-    SolveArgs sa;
-    sa.nrhs = P.nrhs;
-    sa.rtol = P.rtol;
-    sa.inner_rtol = P.inner_rtol;
-    sa.max_outer = P.max_outer;
-    sa.max_inner = P.max_inner;
-    sp_solve_info in = solve_rve<T, K, NT>(g, nsv, pl.nbr, dinv, etype, sKe, sD, sBbar, u, r, x, p,
-                                           q, sa, red, &sh, savg);
-    if (t == 0) {
-      for (int qq = 0; qq < P.nrhs; qq++) {
-        size_t o = ((size_t)rid * P.nrhs + qq) * 6;
-        for (int v = 0; v < 6; v++) {
-          if (P.out_strain) P.out_strain[o + v] = savg[qq * 12 + v];
-          P.out_stress[o + v] = savg[qq * 12 + 6 + v];
-        }
-      }
-      P.out_info[rid] = in;
-    }
-    __syncthreads();
-  }
-}
-
 // ------------------------------------------------------------- dispatch ---
 
-using BatchFn = void (*)(BatchParams);
+SP_BATCH_SHAPES(SP_BATCH_EXTERN, float, 1)
+SP_BATCH_SHAPES(SP_BATCH_EXTERN, float, 6)
+SP_BATCH_SHAPES(SP_BATCH_EXTERN, float, 8)
+SP_BATCH_SHAPES_FP64(SP_BATCH_EXTERN, double, 1)
+SP_BATCH_SHAPES_FP64(SP_BATCH_EXTERN, double, 6)
+SP_BATCH_SHAPES_FP64(SP_BATCH_EXTERN, double, 8)
+
+struct Shape {
+  int threads, ctas, cluster;
+};
 
 template <typename T, int K>
-static BatchFn pick_shape(int threads, int ctas) {
-  if (threads == 256) return ctas >= 4 ? k_batch<T, K, 256, 4> : k_batch<T, K, 256, 2>;
-  return ctas >= 2 ? k_batch<T, K, 512, 2> : k_batch<T, K, 512, 1>;
+static BatchFn pick_shape(const Shape &s) {
+#define SP_BATCH_MATCH(T_, K_, NT, MINB, CL) \
+  if (s.threads == NT && s.ctas == MINB && s.cluster == CL) return k_batch<T_, K_, NT, MINB, CL>;
+  if constexpr (sizeof(T) == 4) {
+    SP_BATCH_SHAPES(SP_BATCH_MATCH, T, K)
+  } else {
+    SP_BATCH_SHAPES_FP64(SP_BATCH_MATCH, T, K)
+  }
+#undef SP_BATCH_MATCH
+  return nullptr;
 }
 
-static BatchFn pick(int prec, int K, int threads, int ctas) {
+static BatchFn pick(int prec, int K, const Shape &s) {
   if (prec == SP_PREC_FP64) {
-    if (K == 1) return pick_shape<double, 1>(threads, ctas);
-    if (K <= 6) return pick_shape<double, 6>(threads, ctas);
-    return pick_shape<double, 8>(threads, ctas);
+    if (K == 1) return pick_shape<double, 1>(s);
+    if (K <= 6) return pick_shape<double, 6>(s);
+    return pick_shape<double, 8>(s);
   }
-  if (K == 1) return pick_shape<float, 1>(threads, ctas);
-  if (K <= 6) return pick_shape<float, 6>(threads, ctas);
-  return pick_shape<float, 8>(threads, ctas);
+  if (K == 1) return pick_shape<float, 1>(s);
+  if (K <= 6) return pick_shape<float, 6>(s);
+  return pick_shape<float, 8>(s);
 }
 
 static int kpad(int nrhs) { return nrhs == 1 ? 1 : (nrhs <= 6 ? 6 : 8); }
@@ -205,6 +98,7 @@ extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   o->threads = 512;
   o->lanes_per_row = 0;
   o->ctas_per_sm = 2;
+  o->cluster = 1;
 }
 
 extern "C" int sp_batch_destroy(sp_batch *b) {
@@ -240,6 +134,9 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (o.threads == 256 && o.ctas_per_sm != 2 && o.ctas_per_sm != 4)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: 256-thread CTAs run 2 or 4 per SM");
   o.lanes_per_row = 0;  // the node-sliced SpMM uses one lane per node (3 rows)
+  if (o.cluster == 0) o.cluster = 1;
+  if (o.cluster != 1 && o.cluster != 2 && o.cluster != 4 && o.cluster != 8)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: cluster must be 1, 2, 4 or 8");
   if (o.max_outer < 1) o.max_outer = 8;
   if (o.max_inner < 1) o.max_inner = 4000;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
@@ -308,7 +205,35 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     return hplans[hrves[a].plan].geo.ndof > hplans[hrves[c].plan].geo.ndof;
   });
   int nrhs = o.nrhs, kp = b->kp;
-  b->grid = d->nsm * o.ctas_per_sm;
+  // persistent grid: as many clusters as can be resident at once
+  {
+    Shape sh{o.threads, o.ctas_per_sm, o.cluster};
+    BatchFn fn = pick(o.precision, kp, sh);
+    if (!fn && !rc)
+      rc = sp_set_error(SP_ERR_ARG, "sp_batch_create: no kernel for %d threads x %d CTAs/SM, "
+                        "cluster %d in this precision", o.threads, o.ctas_per_sm, o.cluster);
+    int g = d->nsm * o.ctas_per_sm;
+    if (o.cluster > 1 && !rc) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(g);
+      cfg.blockDim = dim3(o.threads);
+      cudaLaunchAttribute at;
+      at.id = cudaLaunchAttributeClusterDimension;
+      at.val.clusterDim.x = o.cluster;
+      at.val.clusterDim.y = 1;
+      at.val.clusterDim.z = 1;
+      cfg.attrs = &at;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      if (cudaOccupancyMaxActiveClusters(&ncl, (void *)fn, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: cluster of %d CTAs cannot be resident",
+                          o.cluster);
+      }
+      g = std::min(g, ncl * o.cluster);
+    }
+    b->grid = g;
+  }
   size_t stride = (size_t)kp * 3 * maxnp;
   size_t rm_stride = (size_t)maxdof * SP_WP, drm_stride = (size_t)(maxdof + 3) / 4 * 4;
   size_t *acct = &b->bytes;
@@ -324,10 +249,11 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (!rc) rc = dmalloc((void **)&b->d_stress, (size_t)nrve * nrhs * 6 * sizeof(double), acct);
   if (!rc) rc = dmalloc((void **)&b->d_strain, (size_t)nrve * nrhs * 6 * sizeof(double), acct);
   if (!rc) rc = dmalloc((void **)&b->d_info, (size_t)nrve * sizeof(sp_solve_info), acct);
-  if (!rc) rc = dmalloc((void **)&b->d_ws_u, (size_t)b->grid * stride * sizeof(double), acct);
-  if (!rc) rc = dmalloc(&b->d_ws_v, (size_t)b->grid * 4 * stride * tsz, acct);
-  if (!rc) rc = dmalloc(&b->d_ws_rm, (size_t)b->grid * rm_stride * tsz, acct);
-  if (!rc) rc = dmalloc(&b->d_ws_drm, (size_t)b->grid * drm_stride * tsz, acct);
+  const size_t slots = (size_t)(b->grid / o.cluster);  // one work space per cluster
+  if (!rc) rc = dmalloc((void **)&b->d_ws_u, slots * stride * sizeof(double), acct);
+  if (!rc) rc = dmalloc(&b->d_ws_v, slots * 4 * stride * tsz, acct);
+  if (!rc) rc = dmalloc(&b->d_ws_rm, slots * rm_stride * tsz, acct);
+  if (!rc) rc = dmalloc(&b->d_ws_drm, slots * drm_stride * tsz, acct);
   if (!rc) {
     // default inputs: unit strains e_0..e_{nrhs-1}, materials of the descriptors
     std::vector<double> eps((size_t)nrve * nrhs * 6, 0.0), mats((size_t)nrve * 4);
@@ -410,9 +336,25 @@ extern "C" int sp_batch_launch(sp_batch *b, void *stream) {
   Device *d;
   SP_TRY(device(&d));
   cudaStream_t s = pick_stream(stream, d);
-  BatchFn fn = pick(b->o.precision, b->nrhs, b->o.threads, b->o.ctas_per_sm);
+  Shape sh{b->o.threads, b->o.ctas_per_sm, b->o.cluster};
+  BatchFn fn = pick(b->o.precision, b->nrhs, sh);
   SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
-  fn<<<b->grid, b->o.threads, 0, s>>>(b->P);
+  if (b->o.cluster == 1) {
+    fn<<<b->grid, b->o.threads, 0, s>>>(b->P);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(b->grid);
+    cfg.blockDim = dim3(b->o.threads);
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = b->o.cluster;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    SP_CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, b->P));
+  }
   SP_CUDA_TRY(cudaGetLastError());
   b->last_launches = 1;
   return SP_OK;

@@ -1,0 +1,160 @@
+// rve_batch_kernel.cuh -- the batched persistent kernel (see rve_batch.cu),
+// in a header so that its instantiations compile in parallel translation
+// units (rve_batch_inst_*.cu).
+#pragma once
+
+#include "rve_solve.cuh"
+#include "sp_cuda.h"
+
+namespace sp {
+
+struct BatchPlan {
+  MeshGeo geo; // node/element counts; h and vol per RVE
+  const int *cols;
+  const int *nbr;
+  const uint8_t *slot;
+  const int *color_elems;
+  int color_off[9];
+};
+
+struct BatchRve {
+  int plan, pad;
+  double len[3];
+  long long nsv_off, etype_off, dinv_off;
+};
+
+struct BatchParams {
+  const BatchPlan *plans;
+  const BatchRve *rves;
+  const int *order;
+  int nrve, nrhs;
+  void *nsv;   // float or double pool: node-sliced ELL values per RVE
+  void *dinv;  // float or double pool: component-major Jacobi diagonal per RVE
+  const uint8_t *etype;
+  const double *strains; // [nrve][nrhs][6]
+  const double *mats;    // [nrve][4]
+  double *out_stress;    // [nrve][nrhs][6]
+  double *out_strain;
+  sp_solve_info *out_info;
+  double *ws_u;          // per CTA [K][3][max nn_pad] FP64
+  void *ws_v;            // per CTA 4 x [K][3][max nn_pad] of T: r, x, p, q
+  size_t ws_stride;      // K*3*max nn_pad
+  void *ws_rm;           // per CTA row-major assembly scratch [maxdof][84] of T
+  void *ws_drm;          // per CTA row-major diagonal scratch [maxdof] of T
+  size_t rm_stride;      // maxdof*84
+  size_t drm_stride;     // maxdof rounded up to 4
+  int *counter;
+  double rtol, inner_rtol;
+  int max_outer, max_inner;
+};
+
+template <typename T, int K, int NT, int MINB, int CL>
+__global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
+  __shared__ double sKe[2 * SP_KE];
+  __shared__ T sKeT[2 * SP_KE];
+  __shared__ double sD[72], sBbar[144], sdsh[192];
+  // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
+  __shared__ double red[33 * 16];
+  __shared__ double savg[SP_MAX_RHS * 12];
+  __shared__ CgShared sh;
+  __shared__ int s_job;
+  const int t = threadIdx.x;
+  const int rank = rve_rank<CL>();
+  const int gt = rank * NT + t;
+  constexpr int GNT = CL * NT;
+  const int slot = blockIdx.x / CL;  // work space of this cluster
+  double *u = P.ws_u + (size_t)slot * P.ws_stride;
+  T *ws = reinterpret_cast<T *>(P.ws_v) + (size_t)slot * 4 * P.ws_stride;
+  T *r = ws, *x = ws + P.ws_stride, *p = ws + 2 * P.ws_stride, *q = ws + 3 * P.ws_stride;
+  T *vrm = reinterpret_cast<T *>(P.ws_rm) + (size_t)slot * P.rm_stride;
+  T *drm = reinterpret_cast<T *>(P.ws_drm) + (size_t)slot * P.drm_stride;
+
+  for (;;) {
+    // rank 0 claims the next RVE and hands it to the cluster
+    if (t == 0 && rank == 0) {
+      int job = atomicAdd(P.counter, 1);
+      if constexpr (CL == 1) {
+        s_job = job;
+      } else {
+        cg::cluster_group cl = cg::this_cluster();
+        for (int rr = 0; rr < CL; rr++) *cl.map_shared_rank(&s_job, rr) = job;
+      }
+    }
+    rve_sync<CL>();
+    int job = s_job;
+    rve_sync<CL>();
+    if (job >= P.nrve) break;
+    const int rid = P.order[job];
+    const BatchRve rv = P.rves[rid];
+    const BatchPlan pl = P.plans[rv.plan];
+    MeshGeo g = pl.geo;
+    g.hx = rv.len[0] / g.nex;
+    g.hy = rv.len[1] / g.ney;
+    g.hz = rv.len[2] / g.nez;
+    g.vol = rv.len[0] * rv.len[1] * rv.len[2];
+    T *nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
+    T *dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
+    const uint8_t *etype = P.etype + rv.etype_off;
+
+    // 1. element operators (every CTA keeps its own copy)
+    if (t < 2) iso_D(P.mats[rid * 4 + 2 * t], P.mats[rid * 4 + 2 * t + 1], sD + 36 * t);
+    double h[3] = {g.hx, g.hy, g.hz};
+    elem_ops_stage1(t, NT, h, sdsh);
+    __syncthreads();
+    elem_ops_stage2(t, NT, h, sdsh, sD, 2, sKe, sBbar);
+    __syncthreads();
+    for (int i = t; i < 2 * SP_KE; i += NT) sKeT[i] = (T)sKe[i];
+    // 2. assembly: coloured scatter into the row-major scratch, Dirichlet
+    //    rows/columns, then the node-sliced copy the solve reads
+    ell_zero<T>(gt, GNT, vrm, g.ndof);
+    rve_sync<CL>();
+    for (int c = 0; c < 8; c++) {
+      if (pl.color_off[c + 1] > pl.color_off[c])
+        scatter_colour<T>(gt, GNT, g, pl.color_elems, pl.color_off[c], pl.color_off[c + 1],
+                          pl.slot, etype, sKeT, vrm);
+      rve_sync<CL>();
+    }
+    bc_and_dinv<T>(gt, GNT, g, pl.cols, vrm, drm);
+    rve_sync<CL>();
+    ns_from_rows<T>(gt, GNT, g, pl.cols, vrm, drm, nsv, dinv);
+    // load cases: u = eps . x on the boundary, 0 inside
+    affine_soa<K>(gt, GNT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, false, u);
+    rve_sync<CL>();
+
+    SolveArgs sa;
+    sa.nrhs = P.nrhs;
+    sa.rtol = P.rtol;
+    sa.inner_rtol = P.inner_rtol;
+    sa.max_outer = P.max_outer;
+    sa.max_inner = P.max_inner;
+    sp_solve_info in = solve_rve<T, K, NT, CL>(g, nsv, pl.nbr, dinv, etype, sKe, sD, sBbar, u, r,
+                                               x, p, q, sa, red, &sh, savg);
+    if (t == 0 && rank == 0) {
+      for (int qq = 0; qq < P.nrhs; qq++) {
+        size_t o = ((size_t)rid * P.nrhs + qq) * 6;
+        for (int v = 0; v < 6; v++) {
+          if (P.out_strain) P.out_strain[o + v] = savg[qq * 12 + v];
+          P.out_stress[o + v] = savg[qq * 12 + 6 + v];
+        }
+      }
+      P.out_info[rid] = in;
+    }
+    rve_sync<CL>();
+  }
+}
+
+using BatchFn = void (*)(BatchParams);
+
+// the instantiated shapes: (threads, min CTAs per SM, cluster)
+#define SP_BATCH_SHAPES(X, T, K) \
+  X(T, K, 512, 1, 1) X(T, K, 512, 2, 1) X(T, K, 256, 2, 1) X(T, K, 256, 4, 1) \
+  X(T, K, 512, 1, 2) X(T, K, 512, 2, 2) X(T, K, 512, 1, 4) X(T, K, 512, 2, 4) \
+  X(T, K, 512, 1, 8) X(T, K, 512, 2, 8)
+#define SP_BATCH_SHAPES_FP64(X, T, K) X(T, K, 512, 1, 1) X(T, K, 512, 2, 1)
+
+#define SP_BATCH_EXTERN(T, K, NT, MINB, CL) \
+  extern template __global__ void k_batch<T, K, NT, MINB, CL>(BatchParams);
+#define SP_BATCH_DEFINE(T, K, NT, MINB, CL) \
+  template __global__ void k_batch<T, K, NT, MINB, CL>(BatchParams);
+
+}  // namespace sp

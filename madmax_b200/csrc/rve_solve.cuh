@@ -1,19 +1,28 @@
 // rve_solve.cuh -- the per-RVE solve shared by the batched kernel
-// (rve_batch.cu) and the serving loop (serve.cu), run by one CTA of NT
-// threads: FP64 element residual (micro/src/assembly.c:33-82), Jacobi-PCG
-// corrections in precision T on the RVE's node-sliced ELL values, FP64
-// update of u (micro/src/homogenize.c:184-215, with a relative stopping
-// rule) and FP64 volume averages (micro/src/homogenize.c:344-368).
+// (rve_batch.cu) and the serving loop (serve.cu): FP64 element residual
+// (micro/src/assembly.c:33-82), Jacobi-PCG corrections in precision T on
+// the RVE's node-sliced ELL values, FP64 update of u (micro/src/
+// homogenize.c:184-215, with a relative stopping rule) and FP64 volume
+// averages (micro/src/homogenize.c:344-368).
 //
-// The CG scalars of the K load cases live in shared memory (CgShared) and
-// are updated by warp 0 inside each reduction, so the threads carry no
-// per-load-case state across the loop.  Vectors are component-major,
+// One RVE is solved by a thread-block cluster of CL CTAs of NT threads
+// (CL = 1: a single CTA, no cluster instructions).  Every loop is split over
+// the cluster's CL*NT threads; partial sums are reduced in each CTA, then
+// added across the cluster through distributed shared memory in rank order,
+// so every CTA holds the same totals and computes the same CG scalars
+// (deterministic, independent of scheduling).  Cluster barriers separate
+// the phases in which a CTA reads rows another CTA wrote (the SpMM gathers,
+// the residual gathers of u).  Vectors are component-major,
 // v[(k*3 + d)*nn_pad + node], padding nodes zero.
 #pragma once
+
+#include <cooperative_groups.h>
 
 #include "rve_device.cuh"
 
 namespace sp {
+
+namespace cg = cooperative_groups;
 
 struct SolveArgs {
   int nrhs;
@@ -26,13 +35,34 @@ struct CgShared {
   double alpha[SP_MAX_RHS], beta[SP_MAX_RHS];
   int act[SP_MAX_RHS];
   int nact, done;
+  // cluster reduction: [buffer][rank][value], written by every rank into
+  // rank 0's copy
+  double cpart[2][8][16];
+  int phase;
 };
 
-// Block reduction of NV partial sums; the totals are left in
-// red[32*NV .. 33*NV) for warp 0 (no trailing barrier: the caller's update
-// runs in warp 0 and then synchronises).
-template <int NV>
-__device__ inline void block_reduce_w0(const double *v, double *red) {
+// Barrier over the threads that solve one RVE.
+template <int CL>
+__device__ inline void rve_sync() {
+  if constexpr (CL == 1)
+    __syncthreads();
+  else
+    cg::this_cluster().sync();
+}
+
+template <int CL>
+__device__ inline int rve_rank() {
+  if constexpr (CL == 1)
+    return 0;
+  else
+    return (int)cg::this_cluster().block_rank();
+}
+
+// Sum NV per-thread partials over the CTA (and the cluster).  The totals
+// end in red[32*NV + q] of every CTA, readable by warp 0; no trailing CTA
+// barrier (the caller's warp-0 update follows, then a __syncthreads).
+template <int NV, int CL>
+__device__ inline void rve_reduce(const double *v, double *red, CgShared *sh) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; q++) {
@@ -51,6 +81,23 @@ __device__ inline void block_reduce_w0(const double *v, double *red) {
       if (lane == 0) red[32 * NV + q] = s;
     }
     __syncwarp();
+  }
+  if constexpr (CL > 1) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int ph = sh->phase;
+    if (warp == 0 && lane < NV) {
+      double *dst = cl.map_shared_rank(&sh->cpart[ph][cl.block_rank()][lane], 0);
+      *dst = red[32 * NV + lane];
+    }
+    cl.sync();
+    if (warp == 0 && lane < NV) {
+      const double *src = cl.map_shared_rank(&sh->cpart[ph][0][0], 0);
+      double s = 0.0;
+      for (int r = 0; r < CL; r++) s += src[r * 16 + lane];
+      red[32 * NV + lane] = s;
+    }
+    __syncwarp();
+    if (threadIdx.x == 0) sh->phase = ph ^ 1;
   }
 }
 
@@ -73,10 +120,11 @@ struct V16 {
 };
 
 // On entry u holds the start iterate with the boundary values of every load
-// case.  On exit avg[q*12 + 0..5] = <strain>_q, avg[q*12 + 6..11] =
-// <stress>_q (q < nrhs, shared memory) and the return value describes the
-// solve.  red: shared scratch of 33*16 doubles; sh: shared CG scalars.
-template <typename T, int K, int NT>
+// case (visible to the whole cluster).  On exit avg[q*12 + 0..5] =
+// <strain>_q, avg[q*12 + 6..11] = <stress>_q (q < nrhs, shared memory of
+// every CTA) and the return value describes the solve.  red: shared scratch
+// of 33*16 doubles; sh: shared CG scalars.
+template <typename T, int K, int NT, int CL>
 __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nbr, const T *dinv,
                                    const uint8_t *etype, const double *sKe, const double *sD,
                                    const double *sBbar, double *u, T *r, T *x, T *p, T *q,
@@ -85,22 +133,25 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
   constexpr int E = W::E;
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
+  const int gt = rve_rank<CL>() * NT + t;  // index among the RVE's threads
+  constexpr int GNT = CL * NT;
   const int blk = 3 * g.nn_pad;  // values per load case
   const int nch = blk / E;       // 16-byte chunks per load case
   if (t < SP_MAX_RHS) {
     sh->rn0[t] = 0.0;
     sh->act[t] = 0;
   }
+  if (t == 0) sh->phase = 0;
   int outer = 0, inner = 0;
-  __syncthreads();
+  rve_sync<CL>();
   for (;;) {
     // 3a. FP64 residual b = -K u -> r (type T) and its norms
     {
       double m1[K];
 #pragma unroll
       for (int k = 0; k < K; k++) m1[k] = 0.0;
-      residual_soa<K, T>(t, NT, g, etype, sKe, u, r, m1);
-      block_reduce_w0<K>(m1, red);
+      residual_soa<K, T>(gt, GNT, g, etype, sKe, u, r, m1);
+      rve_reduce<K, CL>(m1, red, sh);
       if (warp == 0) {
         bool notdone = false;
         if (lane < K) {
@@ -127,7 +178,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
       for (int k = 0; k < 2 * K; k++) m2[k] = 0.0;
 #pragma unroll
       for (int k = 0; k < K; k++) {
-        for (int c = t; c < nch; c += NT) {
+        for (int c = gt; c < nch; c += GNT) {
           size_t o = (size_t)k * blk + (size_t)c * E;
           W rv = W::load(r + o), dv = W::load(dinv + (size_t)c * E), zv, zero;
 #pragma unroll
@@ -141,7 +192,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
           zero.store(x + o);
         }
       }
-      block_reduce_w0<2 * K>(m2, red);
+      rve_reduce<2 * K, CL>(m2, red, sh);  // (its cluster barrier also publishes p)
       if (warp == 0) {
         bool a = false;
         if (lane < K) {
@@ -163,8 +214,8 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
         double m3[K];
 #pragma unroll
         for (int k = 0; k < K; k++) m3[k] = 0.0;
-        spmm_ns<T, K, false>(t, NT, g, nsv, nbr, p, q, m3);
-        block_reduce_w0<K>(m3, red);
+        spmm_ns<T, K, false>(gt, GNT, g, nsv, nbr, p, q, m3);
+        rve_reduce<K, CL>(m3, red, sh);
         if (warp == 0 && lane < K) {
           double pq = red[32 * K + lane];
           sh->alpha[lane] = (sh->act[lane] && pq != 0.0) ? sh->rho[lane] / pq : 0.0;
@@ -179,7 +230,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
 #pragma unroll
         for (int k = 0; k < K; k++) {
           const T al = (T)sh->alpha[k];
-          for (int c = t; c < nch; c += NT) {
+          for (int c = gt; c < nch; c += GNT) {
             size_t o = (size_t)k * blk + (size_t)c * E;
             W xv = W::load(x + o), pv = W::load(p + o), rv = W::load(r + o), qv = W::load(q + o);
             W dv = W::load(dinv + (size_t)c * E);
@@ -194,7 +245,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
             rv.store(r + o);
           }
         }
-        block_reduce_w0<2 * K>(m2, red);
+        rve_reduce<2 * K, CL>(m2, red, sh);
         if (warp == 0) {
           bool a = false;
           if (lane < K) {
@@ -216,7 +267,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
 #pragma unroll
       for (int k = 0; k < K; k++) {
         const T be = (T)sh->beta[k];
-        for (int c = t; c < nch; c += NT) {
+        for (int c = gt; c < nch; c += GNT) {
           size_t o = (size_t)k * blk + (size_t)c * E;
           W rv = W::load(r + o), pv = W::load(p + o), dv = W::load(dinv + (size_t)c * E);
 #pragma unroll
@@ -224,29 +275,30 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
           pv.store(p + o);
         }
       }
-      __syncthreads();
+      rve_sync<CL>();  // the next SpMM gathers p rows of every CTA
     }
     inner += it;
     // 3c. u += x in FP64
-    for (int i = t; i < K * blk; i += NT) u[i] += (double)x[i];
-    __syncthreads();
+    for (int i = gt; i < K * blk; i += GNT) u[i] += (double)x[i];
+    rve_sync<CL>();  // the residual gathers u rows of every CTA
     outer++;
   }
 
   // 4. averages per load case
   for (int qq = 0; qq < P.nrhs; qq++) {
-    double acc[12], tot[12];
+    double acc[12];
 #pragma unroll
     for (int v = 0; v < 12; v++) acc[v] = 0.0;
-    average_soa(t, NT, g, etype, sD, sBbar, u, qq, acc);
-    block_sum<12>(acc, red, tot);
+    average_soa(gt, GNT, g, etype, sD, sBbar, u, qq, acc);
+    rve_reduce<12, CL>(acc, red, sh);
     if (t == 0)
-      for (int v = 0; v < 12; v++) avg[qq * 12 + v] = tot[v] / g.vol;
+      for (int v = 0; v < 12; v++) avg[qq * 12 + v] = red[32 * 12 + v] / g.vol;
+    __syncthreads();
   }
   double worst = 0.0;
   for (int k = 0; k < P.nrhs; k++)
     if (sh->rn0[k] > 0.0) worst = fmax(worst, sh->rn[k] / sh->rn0[k]);
-  __syncthreads();
+  rve_sync<CL>();
   sp_solve_info in;
   in.status = (worst <= P.rtol) ? SP_OK : SP_ERR_NOCONV;
   in.outer_its = outer;

@@ -76,12 +76,25 @@ def test_same_result_alone_and_in_mix():
     assert np.array_equal(s_again, s_mix)
 
 
-@pytest.mark.parametrize("threads,ctas", [(512, 1), (512, 2), (256, 2), (256, 4)])
-def test_cta_shapes_agree(threads, ctas):
-    descs = make_descs(9, [5, 3, 6])
-    b = mb.Batch(descs, threads=threads, ctas_per_sm=ctas)
+@pytest.mark.parametrize("threads,ctas,cluster", [(512, 1, 1), (512, 2, 1), (256, 2, 1),
+                                                   (256, 4, 1), (512, 2, 2), (512, 1, 4),
+                                                   (512, 2, 8)])
+def test_cta_shapes_agree(threads, ctas, cluster):
+    """Every CTA shape, and RVEs split over thread-block clusters of 2, 4
+    and 8 CTAs, give the oracle's result."""
+    descs = make_descs(9, [5, 3, 6, 2, 8, 12])
+    b = mb.Batch(descs, threads=threads, ctas_per_sm=ctas, cluster=cluster)
     s, _, info = b.homogenize()
     assert (mb.info_array(info)["status"] == 0).all()
     for i, d in enumerate(descs):
         st = oracle_stress(d, np.eye(6))
         assert np.abs(s[i] - st).max() <= 1e-8 * np.abs(st).max()
+
+
+def test_cluster_result_is_deterministic():
+    descs = make_descs(21, [6, 10, 4])
+    a, _, _ = mb.Batch(descs, cluster=4).homogenize()
+    b, _, _ = mb.Batch(descs, cluster=4).homogenize()
+    c, _, _ = mb.Batch(descs[1:2], cluster=4).homogenize()
+    assert np.array_equal(a, b)
+    assert np.array_equal(a[1], c[0])
