@@ -22,6 +22,7 @@ ELL_ERR_CUDA = 5
 SP_ID_MATRIX, SP_ID_FIBER = 0, 1
 SP_PREC_MIXED, SP_PREC_FP64 = 0, 1
 SP_MAX_RHS = 8
+SP_NOALLOC_MAX_ROWS = 262144
 MAX_ITS, MIN_ERR = 100000, 1.0e-10
 
 _dp = C.POINTER(C.c_double)
@@ -109,6 +110,8 @@ _PROTOS = {
     "sp_ell_dev_mvp": (C.c_int, [_vp, _vp, _vp, _vp]),
     "sp_ell_dev_mvp_host": (C.c_int, [_vp, _dp, _dp]),
     "sp_ell_dev_pcg": (C.c_int, [_vp, _dp, _dp, C.c_double, C.c_int, _ip, _dp]),
+    "sp_ell_pcg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_double, C.c_int,
+                                     _ip, _dp, _vp]),
     "sp_classify": (C.c_int, [C.POINTER(sp_rve_desc), _up]),
     "sp_ell_pattern": (C.c_int, [_ip, _ip]),
     "sp_rve_create": (C.c_int, [C.POINTER(sp_rve_desc), C.POINTER(_vp)]),
