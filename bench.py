@@ -37,9 +37,9 @@ SIZES = (8, 12, 16, 20)
 E_MATRIX = 1e9
 
 
-def workload_params(nrve: int, seed: int):
+def workload_params(nrve: int, seed: int, sizes=SIZES):
     rng = np.random.default_rng(seed)
-    n = rng.choice(SIZES, size=nrve)
+    n = rng.choice(sizes, size=nrve)
     radius = rng.uniform(0.1, 0.35, size=nrve)
     ratio = np.exp(rng.uniform(np.log(2.0), np.log(100.0), size=nrve))
     nu_m = rng.uniform(0.2, 0.35, size=nrve)
@@ -47,8 +47,8 @@ def workload_params(nrve: int, seed: int):
     return n, radius, ratio, nu_m, nu_f
 
 
-def workload_descs(mb, nrve: int, seed: int):
-    n, radius, ratio, nu_m, nu_f = workload_params(nrve, seed)
+def workload_descs(mb, nrve: int, seed: int, sizes=SIZES):
+    n, radius, ratio, nu_m, nu_f = workload_params(nrve, seed, sizes)
     return [mb.rve_desc(int(n[i]), float(radius[i]), (E_MATRIX, E_MATRIX * float(ratio[i])),
                         (float(nu_m[i]), float(nu_f[i]))) for i in range(nrve)]
 
@@ -233,11 +233,11 @@ def run_ours(args):
     sptr = C.c_void_p(stream.cuda_stream)
     assert sptr.value, "expected a non-default stream"
 
-    descs = workload_descs(mb, args.nrve, 1234 + rank)
+    descs = workload_descs(mb, args.nrve, 1234 + rank, tuple(args.sizes))
     sizes = [d.n[0] for d in descs]
     t0 = time.time()
     batch = mb.Batch(descs, nrhs=6, threads=args.threads, ctas_per_sm=args.ctas,
-                     cluster=args.cluster)
+                     cluster=args.cluster, inner_rtol=args.inner_rtol)
     setup_s = time.time() - t0
 
     for _ in range(args.warmup):
@@ -315,10 +315,10 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 CG + f64 refinement", "data": "synthetic",
             "config": {"workload": f"batched tangent: {args.nrve} RVEs per GPU, n uniform in "
-                                   "{8,12,16,20}, 6 unit-strain load cases, rtol 1e-8",
+                                   f"{set(args.sizes)}, 6 unit-strain load cases, rtol 1e-8",
                        "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8,
                        "precision": "mixed", "cta_threads": args.threads, "ctas_per_sm": args.ctas,
-                       "cluster": args.cluster,
+                       "cluster": args.cluster, "inner_rtol": args.inner_rtol,
                        "l2": "inputs larger than L2 (FP32 ELL values alone are "
                              f"{sum(3 * (n + 1) ** 3 * 84 * 4 for n in sizes) / 1e9:.1f} GB)",
                        "parallelism": f"replicas x{world} (independent RVEs per rank)"},
@@ -463,6 +463,9 @@ def main(argv=None):
     ap.add_argument("--threads", type=int, default=512)
     ap.add_argument("--ctas", type=int, default=2)
     ap.add_argument("--cluster", type=int, default=1)
+    ap.add_argument("--inner-rtol", type=float, default=1e-4)
+    ap.add_argument("--sizes", type=int, nargs="+", default=list(SIZES),
+                    help="mesh sizes to draw from (the headline workload uses 8 12 16 20)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--plain-per-size", type=int, default=2)
     ap.add_argument("--cpu-sample", type=int, default=8)

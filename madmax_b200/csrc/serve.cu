@@ -36,7 +36,7 @@
 namespace sp {
 
 constexpr int SERVE_NT = 512;
-constexpr int SERVE_K = 8;  // 7 load cases + 1 idle slot
+constexpr int SERVE_K = 7;  // eps and eps + delta e_i, i = 0..5 (component-major vectors need no padding)
 constexpr int SERVE_NRHS = 7;
 constexpr double FD_DELTA = 0.005;  // micro/inc/micro.h:29
 
@@ -330,7 +330,7 @@ extern "C" void sp_server_opts_default(sp_server_opts *o) {
   o->max_inflight = 0;
   o->queue_capacity = 65536;
   o->rtol = 1e-8;
-  o->inner_rtol = 1e-5;
+  o->inner_rtol = 1e-4;
   o->idle_spin_limit = 2000000;
 }
 
@@ -403,7 +403,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   if (opts) o = *opts; else sp_server_opts_default(&o);
   if (o.queue_capacity <= 0) o.queue_capacity = 65536;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
-  if (!(o.inner_rtol > 0)) o.inner_rtol = 1e-5;
+  if (!(o.inner_rtol > 0)) o.inner_rtol = 1e-4;
   if (o.idle_spin_limit <= 0) o.idle_spin_limit = 2000000;
   Device *d;
   SP_TRY(device(&d));
