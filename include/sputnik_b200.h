@@ -156,6 +156,10 @@ int sp_rve_tangent(sp_rve *r, double rtol, double *C, sp_solve_info *info);
 #define SP_PREC_MIXED 0 /* FP32 ELL values + FP32 CG, FP64 residual refinement */
 #define SP_PREC_FP64 1  /* FP64 values and CG */
 
+#define SP_OP_ELL 0     /* inner CG on the RVE's assembled ELL values (coloured scatter) */
+#define SP_OP_STENCIL 1 /* inner CG on the element-type stencil: A p from the two element
+                           stiffnesses and the element materials, no matrix in memory */
+
 typedef struct {
   int nrhs;          /* load cases per RVE, 1..8 (default 6) */
   int precision;     /* SP_PREC_MIXED (default) or SP_PREC_FP64 */
@@ -166,7 +170,8 @@ typedef struct {
   int threads;       /* threads per CTA (0: tuned) */
   int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
   int ctas_per_sm;   /* resident CTAs per SM: 1 or 2 (512 threads), 2 or 4 (256) */
-  int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 */
+  int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 (assembled) */
+  int op;            /* SP_OP_STENCIL (default) or SP_OP_ELL */
 } sp_batch_opts;
 
 void sp_batch_opts_default(sp_batch_opts *o);

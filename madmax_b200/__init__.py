@@ -21,6 +21,7 @@ SP_ERR_CUDA, SP_ERR_NOCONV, SP_ERR_BUDGET, SP_ERR_TIMEOUT, SP_ERR_STATE, SP_PEND
 ELL_ERR_CUDA = 5
 SP_ID_MATRIX, SP_ID_FIBER = 0, 1
 SP_PREC_MIXED, SP_PREC_FP64 = 0, 1
+SP_OP_ELL, SP_OP_STENCIL = 0, 1
 SP_MAX_RHS = 8
 SP_NOALLOC_MAX_ROWS = 262144
 MAX_ITS, MIN_ERR = 100000, 1.0e-10
@@ -64,7 +65,7 @@ class sp_batch_opts(C.Structure):
     _fields_ = [("nrhs", C.c_int), ("precision", C.c_int), ("rtol", C.c_double),
                 ("inner_rtol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
                 ("threads", C.c_int), ("lanes_per_row", C.c_int), ("ctas_per_sm", C.c_int),
-                ("cluster", C.c_int)]
+                ("cluster", C.c_int), ("op", C.c_int)]
 
 
 class sp_server_opts(C.Structure):
@@ -329,7 +330,10 @@ class Rve:
 def batch_opts(**kw) -> sp_batch_opts:
     o = sp_batch_opts()
     lib().sp_batch_opts_default(C.byref(o))
+    names = {f[0] for f in sp_batch_opts._fields_}
     for k, v in kw.items():
+        if k not in names:
+            raise TypeError(f"unknown batch option {k!r}")
         setattr(o, k, v)
     return o
 

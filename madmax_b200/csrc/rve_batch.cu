@@ -36,13 +36,14 @@ SP_BATCH_SHAPES_FP64(SP_BATCH_EXTERN, double, 6)
 SP_BATCH_SHAPES_FP64(SP_BATCH_EXTERN, double, 8)
 
 struct Shape {
-  int threads, ctas, cluster;
+  int threads, ctas, cluster, op;
 };
 
 template <typename T, int K>
 static BatchFn pick_shape(const Shape &s) {
-#define SP_BATCH_MATCH(T_, K_, NT, MINB, CL) \
-  if (s.threads == NT && s.ctas == MINB && s.cluster == CL) return k_batch<T_, K_, NT, MINB, CL>;
+#define SP_BATCH_MATCH(T_, K_, NT, MINB, CL, OP) \
+  if (s.threads == NT && s.ctas == MINB && s.cluster == CL && s.op == OP) \
+    return k_batch<T_, K_, NT, MINB, CL, OP>;
   if constexpr (sizeof(T) == 4) {
     SP_BATCH_SHAPES(SP_BATCH_MATCH, T, K)
   } else {
@@ -83,7 +84,7 @@ struct sp_batch_s {
   double *d_strains = nullptr, *d_mats = nullptr, *d_stress = nullptr, *d_strain = nullptr;
   sp_solve_info *d_info = nullptr;
   double *d_ws_u = nullptr;
-  void *d_ws_v = nullptr, *d_ws_rm = nullptr, *d_ws_drm = nullptr;
+  void *d_ws_v = nullptr, *d_ws_rm = nullptr, *d_ws_drm = nullptr, *d_ws_dinv = nullptr;
   size_t bytes = 0;
 };
 
@@ -99,13 +100,14 @@ extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   o->lanes_per_row = 0;
   o->ctas_per_sm = 2;
   o->cluster = 1;
+  o->op = SP_OP_STENCIL;
 }
 
 extern "C" int sp_batch_destroy(sp_batch *b) {
   if (!b) return SP_OK;
   void *bufs[] = {b->d_plans, b->d_rves, b->d_order, b->d_counter, b->d_vals, b->d_dinv,
                   b->d_etype, b->d_strains, b->d_mats, b->d_stress, b->d_strain, b->d_info,
-                  b->d_ws_u, b->d_ws_v, b->d_ws_rm, b->d_ws_drm};
+                  b->d_ws_u, b->d_ws_v, b->d_ws_rm, b->d_ws_drm, b->d_ws_dinv};
   for (void *p : bufs) cudaFree(p);
   for (DevPlan *p : b->plans) plan_release(p);
   delete b;
@@ -137,6 +139,8 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (o.cluster == 0) o.cluster = 1;
   if (o.cluster != 1 && o.cluster != 2 && o.cluster != 4 && o.cluster != 8)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: cluster must be 1, 2, 4 or 8");
+  if (o.op != SP_OP_ELL && o.op != SP_OP_STENCIL)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown operator");
   if (o.max_outer < 1) o.max_outer = 8;
   if (o.max_inner < 1) o.max_inner = 4000;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
@@ -187,9 +191,11 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     r.nsv_off = voff;
     r.etype_off = eoff;
     r.dinv_off = doff;
-    voff += (long long)g.nn_pad * 243;
     eoff += (g.nelm + 15) / 16 * 16;
-    doff += 3LL * g.nn_pad;
+    if (o.op == SP_OP_ELL) {  // assembled values and diagonal kept per RVE
+      voff += (long long)g.nn_pad * 243;
+      doff += 3LL * g.nn_pad;
+    }
     maxdof = std::max(maxdof, g.ndof);
     maxnp = std::max(maxnp, g.nn_pad);
   }
@@ -207,11 +213,12 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   int nrhs = o.nrhs, kp = b->kp;
   // persistent grid: as many clusters as can be resident at once
   {
-    Shape sh{o.threads, o.ctas_per_sm, o.cluster};
+    Shape sh{o.threads, o.ctas_per_sm, o.cluster, o.op};
     BatchFn fn = pick(o.precision, kp, sh);
     if (!fn && !rc)
       rc = sp_set_error(SP_ERR_ARG, "sp_batch_create: no kernel for %d threads x %d CTAs/SM, "
-                        "cluster %d in this precision", o.threads, o.ctas_per_sm, o.cluster);
+                        "cluster %d, %s operator in this precision", o.threads, o.ctas_per_sm,
+                        o.cluster, o.op == SP_OP_ELL ? "assembled" : "stencil");
     int g = d->nsm * o.ctas_per_sm;
     if (o.cluster > 1 && !rc) {
       cudaLaunchConfig_t cfg = {};
@@ -235,14 +242,16 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     b->grid = g;
   }
   size_t stride = (size_t)kp * 3 * maxnp;
-  size_t rm_stride = (size_t)maxdof * SP_WP, drm_stride = (size_t)(maxdof + 3) / 4 * 4;
+  // (3*maxnp >= maxdof; a multiple of 96, so every slot starts 16-byte aligned)
+  size_t rm_stride = (size_t)maxdof * SP_WP, drm_stride = (size_t)3 * maxnp;
+  const bool ell = o.op == SP_OP_ELL;
   size_t *acct = &b->bytes;
   if (!rc) rc = dmalloc((void **)&b->d_plans, hplans.size() * sizeof(BatchPlan), acct);
   if (!rc) rc = dmalloc((void **)&b->d_rves, nrve * sizeof(BatchRve), acct);
   if (!rc) rc = dmalloc((void **)&b->d_order, nrve * sizeof(int), acct);
   if (!rc) rc = dmalloc((void **)&b->d_counter, 256, acct);
-  if (!rc) rc = dmalloc(&b->d_vals, (size_t)voff * tsz, acct);
-  if (!rc) rc = dmalloc(&b->d_dinv, (size_t)doff * tsz, acct);
+  if (!rc && ell) rc = dmalloc(&b->d_vals, (size_t)voff * tsz, acct);
+  if (!rc && ell) rc = dmalloc(&b->d_dinv, (size_t)doff * tsz, acct);
   if (!rc) rc = dmalloc((void **)&b->d_etype, eoff, acct);
   if (!rc) rc = dmalloc((void **)&b->d_strains, (size_t)nrve * nrhs * 6 * sizeof(double), acct);
   if (!rc) rc = dmalloc((void **)&b->d_mats, (size_t)nrve * 4 * sizeof(double), acct);
@@ -252,8 +261,10 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   const size_t slots = (size_t)(b->grid / o.cluster);  // one work space per cluster
   if (!rc) rc = dmalloc((void **)&b->d_ws_u, slots * stride * sizeof(double), acct);
   if (!rc) rc = dmalloc(&b->d_ws_v, slots * 4 * stride * tsz, acct);
-  if (!rc) rc = dmalloc(&b->d_ws_rm, slots * rm_stride * tsz, acct);
-  if (!rc) rc = dmalloc(&b->d_ws_drm, slots * drm_stride * tsz, acct);
+  if (!rc && ell) rc = dmalloc(&b->d_ws_rm, slots * rm_stride * tsz, acct);
+  if (!rc && ell) rc = dmalloc(&b->d_ws_drm, slots * drm_stride * tsz, acct);
+  // stencil: one Jacobi diagonal [3][max nn_pad] per work space
+  if (!rc && !ell) rc = dmalloc(&b->d_ws_dinv, slots * drm_stride * tsz, acct);
   if (!rc) {
     // default inputs: unit strains e_0..e_{nrhs-1}, materials of the descriptors
     std::vector<double> eps((size_t)nrve * nrhs * 6, 0.0), mats((size_t)nrve * 4);
@@ -299,6 +310,7 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   P.ws_drm = b->d_ws_drm;
   P.rm_stride = rm_stride;
   P.drm_stride = drm_stride;
+  P.ws_dinv = b->d_ws_dinv;
   P.counter = b->d_counter;
   P.rtol = o.rtol;
   P.inner_rtol = o.inner_rtol;
@@ -336,7 +348,7 @@ extern "C" int sp_batch_launch(sp_batch *b, void *stream) {
   Device *d;
   SP_TRY(device(&d));
   cudaStream_t s = pick_stream(stream, d);
-  Shape sh{b->o.threads, b->o.ctas_per_sm, b->o.cluster};
+  Shape sh{b->o.threads, b->o.ctas_per_sm, b->o.cluster, b->o.op};
   BatchFn fn = pick(b->o.precision, b->nrhs, sh);
   SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
   if (b->o.cluster == 1) {

@@ -42,16 +42,19 @@ struct BatchParams {
   void *ws_rm;           // per CTA row-major assembly scratch [maxdof][84] of T
   void *ws_drm;          // per CTA row-major diagonal scratch [maxdof] of T
   size_t rm_stride;      // maxdof*84
-  size_t drm_stride;     // maxdof rounded up to 4
+  size_t drm_stride;     // 3*max nn_pad
+  void *ws_dinv;         // stencil operator: per CTA Jacobi diagonal [3][max nn_pad] of T
   int *counter;
   double rtol, inner_rtol;
   int max_outer, max_inner;
 };
 
-template <typename T, int K, int NT, int MINB, int CL>
+template <typename T, int K, int NT, int MINB, int CL, int OP>
 __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
+  constexpr bool STENCIL = OP == SP_OP_STENCIL;
   __shared__ double sKe[2 * SP_KE];
-  __shared__ T sKeT[2 * SP_KE];
+  // element scatter values (assembled operator) or element blocks (stencil)
+  __shared__ __align__(16) T sKeT[STENCIL ? 2 * SP_KB_TYPE : 2 * SP_KE];
   __shared__ double sD[72], sBbar[144], sdsh[192];
   // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
   __shared__ double red[33 * 16];
@@ -92,8 +95,6 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     g.hy = rv.len[1] / g.ney;
     g.hz = rv.len[2] / g.nez;
     g.vol = rv.len[0] * rv.len[1] * rv.len[2];
-    T *nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
-    T *dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
     const uint8_t *etype = P.etype + rv.etype_off;
 
     // 1. element operators (every CTA keeps its own copy)
@@ -103,20 +104,30 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     __syncthreads();
     elem_ops_stage2(t, NT, h, sdsh, sD, 2, sKe, sBbar);
     __syncthreads();
-    for (int i = t; i < 2 * SP_KE; i += NT) sKeT[i] = (T)sKe[i];
-    // 2. assembly: coloured scatter into the row-major scratch, Dirichlet
-    //    rows/columns, then the node-sliced copy the solve reads
-    ell_zero<T>(gt, GNT, vrm, g.ndof);
-    rve_sync<CL>();
-    for (int c = 0; c < 8; c++) {
-      if (pl.color_off[c + 1] > pl.color_off[c])
-        scatter_colour<T>(gt, GNT, g, pl.color_elems, pl.color_off[c], pl.color_off[c + 1],
-                          pl.slot, etype, sKeT, vrm);
+    T *nsv = nullptr, *dinv;
+    if constexpr (STENCIL) {
+      // 2s. no assembly: the 3x3 element blocks and the Jacobi diagonal
+      dinv = reinterpret_cast<T *>(P.ws_dinv) + (size_t)slot * P.drm_stride;
+      stencil_blocks<T>(t, NT, sKe, sKeT);
+      stencil_dinv<T>(gt, GNT, g, etype, sKe, dinv);
+    } else {
+      nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
+      dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
+      for (int i = t; i < 2 * SP_KE; i += NT) sKeT[i] = (T)sKe[i];
+      // 2. assembly: coloured scatter into the row-major scratch, Dirichlet
+      //    rows/columns, then the node-sliced copy the solve reads
+      ell_zero<T>(gt, GNT, vrm, g.ndof);
       rve_sync<CL>();
+      for (int c = 0; c < 8; c++) {
+        if (pl.color_off[c + 1] > pl.color_off[c])
+          scatter_colour<T>(gt, GNT, g, pl.color_elems, pl.color_off[c], pl.color_off[c + 1],
+                            pl.slot, etype, sKeT, vrm);
+        rve_sync<CL>();
+      }
+      bc_and_dinv<T>(gt, GNT, g, pl.cols, vrm, drm);
+      rve_sync<CL>();
+      ns_from_rows<T>(gt, GNT, g, pl.cols, vrm, drm, nsv, dinv);
     }
-    bc_and_dinv<T>(gt, GNT, g, pl.cols, vrm, drm);
-    rve_sync<CL>();
-    ns_from_rows<T>(gt, GNT, g, pl.cols, vrm, drm, nsv, dinv);
     // load cases: u = eps . x on the boundary, 0 inside
     affine_soa<K>(gt, GNT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, false, u);
     rve_sync<CL>();
@@ -127,8 +138,16 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
-    sp_solve_info in = solve_rve<T, K, NT, CL>(g, nsv, pl.nbr, dinv, etype, sKe, sD, sBbar, u, r,
-                                               x, p, q, sa, red, &sh, savg);
+    sp_solve_info in;
+    if constexpr (STENCIL) {
+      StencilOp<T, K> op{sKeT, etype};
+      in = solve_rve<T, K, NT, CL>(g, op, dinv, etype, sKe, sD, sBbar, u, r, x, p, q, sa, red,
+                                   &sh, savg);
+    } else {
+      EllOp<T, K> op{nsv, pl.nbr};
+      in = solve_rve<T, K, NT, CL>(g, op, dinv, etype, sKe, sD, sBbar, u, r, x, p, q, sa, red,
+                                   &sh, savg);
+    }
     if (t == 0 && rank == 0) {
       for (int qq = 0; qq < P.nrhs; qq++) {
         size_t o = ((size_t)rid * P.nrhs + qq) * 6;
@@ -145,16 +164,21 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
 
 using BatchFn = void (*)(BatchParams);
 
-// the instantiated shapes: (threads, min CTAs per SM, cluster)
+// the instantiated shapes: (threads, min CTAs per SM, cluster, operator)
 #define SP_BATCH_SHAPES(X, T, K) \
-  X(T, K, 512, 1, 1) X(T, K, 512, 2, 1) X(T, K, 256, 2, 1) X(T, K, 256, 4, 1) \
-  X(T, K, 512, 1, 2) X(T, K, 512, 2, 2) X(T, K, 512, 1, 4) X(T, K, 512, 2, 4) \
-  X(T, K, 512, 1, 8) X(T, K, 512, 2, 8)
-#define SP_BATCH_SHAPES_FP64(X, T, K) X(T, K, 512, 1, 1) X(T, K, 512, 2, 1)
+  X(T, K, 512, 1, 1, SP_OP_ELL) X(T, K, 512, 2, 1, SP_OP_ELL) X(T, K, 256, 2, 1, SP_OP_ELL) \
+  X(T, K, 256, 4, 1, SP_OP_ELL) X(T, K, 512, 1, 2, SP_OP_ELL) X(T, K, 512, 2, 2, SP_OP_ELL) \
+  X(T, K, 512, 1, 4, SP_OP_ELL) X(T, K, 512, 2, 4, SP_OP_ELL) X(T, K, 512, 1, 8, SP_OP_ELL) \
+  X(T, K, 512, 2, 8, SP_OP_ELL) \
+  X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL) \
+  X(T, K, 256, 2, 1, SP_OP_STENCIL) X(T, K, 256, 4, 1, SP_OP_STENCIL)
+#define SP_BATCH_SHAPES_FP64(X, T, K) \
+  X(T, K, 512, 1, 1, SP_OP_ELL) X(T, K, 512, 2, 1, SP_OP_ELL) \
+  X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL)
 
-#define SP_BATCH_EXTERN(T, K, NT, MINB, CL) \
-  extern template __global__ void k_batch<T, K, NT, MINB, CL>(BatchParams);
-#define SP_BATCH_DEFINE(T, K, NT, MINB, CL) \
-  template __global__ void k_batch<T, K, NT, MINB, CL>(BatchParams);
+#define SP_BATCH_EXTERN(T, K, NT, MINB, CL, OP) \
+  extern template __global__ void k_batch<T, K, NT, MINB, CL, OP>(BatchParams);
+#define SP_BATCH_DEFINE(T, K, NT, MINB, CL, OP) \
+  template __global__ void k_batch<T, K, NT, MINB, CL, OP>(BatchParams);
 
 }  // namespace sp

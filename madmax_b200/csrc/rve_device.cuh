@@ -628,6 +628,153 @@ __device__ inline void spmm_ns(int t, int nt, const MeshGeo &g, const T *__restr
   }
 }
 
+// ------------------------------------------------ element-type stencil ---
+//
+// Every element of the structured RVE mesh has the same shape, so its
+// assembled matrix is fixed by the element stiffnesses of the two materials
+// and the material id of each element.  The stencil operator applies A x
+// without reading an assembled matrix: for an interior node a and each of
+// its 27 neighbours b it sums the 3x3 block
+//   A_ab = sum over the elements e holding both a and b of Ke[type(e)][a_e][b_e]
+// from shared-memory copies of the two Ke, then multiplies the block into the
+// K right-hand sides.  Only interior nodes are computed.  Dirichlet rows are
+// the identity and Dirichlet columns zero in the assembled matrix; the CG
+// vectors are zero on boundary nodes, so a boundary row of A p is 0 and a
+// boundary column contributes 0, which is what this operator gives when the
+// caller keeps y zero on boundary nodes.
+
+// hexa8 local node index of the element corner (cx, cy, cz) (node order of
+// src/fem.c:324-362)
+__host__ __device__ constexpr int hex8_local(int cx, int cy, int cz) {
+  return cz * 4 + (cy == 0 ? (cx ? 1 : 0) : (cx ? 2 : 3));
+}
+
+constexpr int SP_KB_BLK = 12;                 // padded 3x3 block (16-byte rows for float)
+constexpr int SP_KB_TYPE = 64 * SP_KB_BLK;    // blocks of one material
+
+// KB[ty][(la*8 + lb)*12 + 3d + c] = Ke[ty][3la + d][3lb + c] in T, pads 0
+template <typename T>
+__device__ inline void stencil_blocks(int t, int nt, const double *Ke /*[2][576]*/, T *KB) {
+  for (int x = t; x < 2 * SP_KB_TYPE; x += nt) {
+    int ty = x / SP_KB_TYPE, r = x % SP_KB_TYPE, b = r / SP_KB_BLK, w = r % SP_KB_BLK;
+    int la = b / 8, lb = b % 8;
+    KB[x] = (w < 9) ? (T)Ke[ty * SP_KE + (3 * la + w / 3) * SP_NC + 3 * lb + w % 3] : T(0);
+  }
+}
+
+// Jacobi diagonal inverse of the stencil operator, component-major: for an
+// interior node 1 / sum over its 8 elements of Ke[type][3la+d][3la+d]
+// (summed in FP64, rounded once); 0 on boundary and padding nodes.
+template <typename T>
+__device__ inline void stencil_dinv(int t, int nt, const MeshGeo &g,
+                                    const uint8_t *__restrict__ etype, const double *Ke, T *dinv) {
+  for (int x = t; x < 3 * g.nn_pad; x += nt) {
+    int d = x / g.nn_pad, node = x % g.nn_pad;
+    T v = T(0);
+    if (node < g.nn && !is_bnode(g, node)) {
+      int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
+      double s = 0.0;
+      for (int c = 0; c < 8; c++) {
+        int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+        int e = (i - 1 + ox) + (j - 1 + oy) * g.nex + (k - 1 + oz) * g.nex * g.ney;
+        int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+        s += Ke[etype[e] * SP_KE + (3 * la + d) * SP_NC + 3 * la + d];
+      }
+      v = (T)(1.0 / s);
+    }
+    dinv[x] = v;
+  }
+}
+
+// y = A x (K right-hand sides, component-major) with the stencil operator on
+// interior nodes; boundary and padding entries of y are not written.  A warp
+// takes 32 consecutive interior nodes (x fastest), a lane one node.  Adds
+// x.y per load case into dot[K].
+template <typename T, int K>
+__device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB,
+                                    const uint8_t *__restrict__ etype, const T *x, T *y,
+                                    double *dot) {
+  using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
+  constexpr int BW = SP_KB_BLK * (int)sizeof(T) / 16;  // 16-byte words per block
+  const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
+  const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
+  const int ni = mx * my * mz;
+  const int sy = g.nx, sz = g.nx * g.ny, esy = g.nex, esz = g.nex * g.ney;
+  const size_t blk = (size_t)3 * g.nn_pad;
+  for (int s0 = warp * 32; s0 < ni; s0 += nwarps * 32) {
+    const int id = s0 + lane;
+    const bool valid = id < ni;
+    const int idc = valid ? id : ni - 1;
+    const int i = 1 + idc % mx, j = 1 + (idc / mx) % my, k = 1 + idc / (mx * my);
+    const int a = i + j * sy + k * sz;
+    const int e0 = (i - 1) + (j - 1) * esy + (k - 1) * esz;
+    int tb[8];  // offset of the element's material blocks in KB
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      tb[c] = (int)__ldg(etype + e0 + (c & 1) + ((c >> 1) & 1) * esy + (c >> 2) * esz) *
+              SP_KB_TYPE;
+    A acc[3][K];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int q = 0; q < K; q++) acc[d][q] = A(0);
+    // neighbour planes dz = -1, 0, 1 in turn (a rolled loop bounds the live
+    // registers); within a plane the 9 neighbours and their elements unroll
+#pragma unroll 1
+    for (int dz = -1; dz <= 1; dz++) {
+#pragma unroll
+      for (int m = 0; m < 9; m++) {
+        const int dx = m % 3 - 1, dy = m / 3 - 1;
+        A bv[9];
+#pragma unroll
+        for (int w = 0; w < 9; w++) bv[w] = A(0);
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+          const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+          const int bx = 1 - ox + dx, by = 1 - oy + dy;
+          if (bx < 0 || bx > 1 || by < 0 || by > 1) continue;  // resolved at compile time
+          const int bz = 1 - oz + dz;                            // warp-uniform
+          if (bz < 0 || bz > 1) continue;
+          const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+          const int lb = hex8_local(bx, by, 0) + 4 * bz;
+          const int4 *src =
+              reinterpret_cast<const int4 *>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK);
+          T w[SP_KB_BLK];
+#pragma unroll
+          for (int q = 0; q < BW; q++) {
+            int4 v = src[q];
+            memcpy(reinterpret_cast<char *>(w) + 16 * q, &v, 16);
+          }
+#pragma unroll
+          for (int u = 0; u < 9; u++) bv[u] += (A)w[u];
+        }
+        const int nb = a + dx + dy * sy + dz * sz;
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+          A xb[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) xb[c] = (A)x[q * blk + (size_t)c * g.nn_pad + nb];
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) acc[d][q] = fma(bv[d * 3 + c], xb[c], acc[d][q]);
+        }
+      }
+    }
+    if (valid) {
+#pragma unroll
+      for (int q = 0; q < K; q++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          size_t o = q * blk + (size_t)d * g.nn_pad + a;
+          T yv = (T)acc[d][q];
+          dot[q] += (double)yv * (double)x[o];
+          y[o] = yv;
+        }
+    }
+  }
+}
+
 // b = -K u on interior dofs, 0 on the boundary and on padding (component-
 // major vectors; see residual_nodes for the arithmetic).
 template <int K, typename R>

@@ -1,7 +1,7 @@
 // rve_solve.cuh -- the per-RVE solve shared by the batched kernel
 // (rve_batch.cu) and the serving loop (serve.cu): FP64 element residual
 // (micro/src/assembly.c:33-82), Jacobi-PCG corrections in precision T on
-// the RVE's node-sliced ELL values, FP64 update of u (micro/src/
+// the RVE's operator (assembled or stencil), FP64 update of u (micro/src/
 // homogenize.c:184-215, with a relative stopping rule) and FP64 volume
 // averages (micro/src/homogenize.c:344-368).
 //
@@ -101,6 +101,27 @@ __device__ inline void rve_reduce(const double *v, double *red, CgShared *sh) {
   }
 }
 
+// The two operators the inner CG can apply: the node-sliced copy of the
+// RVE's assembled ELL values, or the element-type stencil (no matrix in
+// memory).  apply() computes q = A p and adds p.q per load case into dot.
+template <typename T, int K>
+struct EllOp {
+  const T *nsv;
+  const int *nbr;
+  __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot) const {
+    spmm_ns<T, K, false>(gt, gnt, g, nsv, nbr, p, q, dot);
+  }
+};
+
+template <typename T, int K>
+struct StencilOp {
+  const T *kb;  // shared-memory element blocks (stencil_blocks)
+  const uint8_t *etype;
+  __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot) const {
+    spmm_stencil<T, K>(gt, gnt, g, kb, etype, p, q, dot);
+  }
+};
+
 // 16-byte vector of T
 template <typename T>
 struct V16 {
@@ -124,8 +145,8 @@ struct V16 {
 // <strain>_q, avg[q*12 + 6..11] = <stress>_q (q < nrhs, shared memory of
 // every CTA) and the return value describes the solve.  red: shared scratch
 // of 33*16 doubles; sh: shared CG scalars.
-template <typename T, int K, int NT, int CL>
-__device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nbr, const T *dinv,
+template <typename T, int K, int NT, int CL, typename Op>
+__device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv,
                                    const uint8_t *etype, const double *sKe, const double *sD,
                                    const double *sBbar, double *u, T *r, T *x, T *p, T *q,
                                    const SolveArgs &P, double *red, CgShared *sh, double *avg) {
@@ -190,6 +211,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
           }
           zv.store(p + o);
           zero.store(x + o);
+          zero.store(q + o);  // (entries an operator does not write stay 0)
         }
       }
       rve_reduce<2 * K, CL>(m2, red, sh);  // (its cluster barrier also publishes p)
@@ -214,7 +236,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const T *nsv, const int *nb
         double m3[K];
 #pragma unroll
         for (int k = 0; k < K; k++) m3[k] = 0.0;
-        spmm_ns<T, K, false>(gt, GNT, g, nsv, nbr, p, q, m3);
+        op.apply(gt, GNT, g, p, q, m3);
         rve_reduce<K, CL>(m3, red, sh);
         if (warp == 0 && lane < K) {
           double pq = red[32 * K + lane];

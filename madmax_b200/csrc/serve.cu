@@ -263,8 +263,9 @@ __global__ void __launch_bounds__(SERVE_NT, 2) k_serve(ServeParams P) {
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
+    EllOp<float, SERVE_K> op{G.vals, G.nbr};
     sp_solve_info in = solve_rve<float, SERVE_K, SERVE_NT, 1>(
-        g, G.vals, G.nbr, G.dinv, G.etype, sKe, sD, sB, u, r, x, p, q, sa, red, &sh, savg);
+        g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p, q, sa, red, &sh, savg);
     // keep this solution as the geometry's next warm start
     for (size_t i = t; i < nu; i += SERVE_NT) __stcg(G.warm + i, u[i]);
     __threadfence();

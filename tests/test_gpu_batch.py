@@ -31,11 +31,13 @@ def oracle_stress(d, strains):
     return st
 
 
+@pytest.mark.parametrize("op", [mb.SP_OP_STENCIL, mb.SP_OP_ELL])
 @pytest.mark.parametrize("precision", [mb.SP_PREC_MIXED, mb.SP_PREC_FP64])
-def test_batch_unit_tangents_match_oracle(precision):
+def test_batch_unit_tangents_match_oracle(precision, op):
+    """Both inner operators: the element-type stencil and the assembled ELL."""
     sizes = [2, 3, 4, 5, 6, 8, 3, 7, 4, 6, 5, 2]
     descs = make_descs(42, sizes)
-    b = mb.Batch(descs, precision=precision)
+    b = mb.Batch(descs, precision=precision, op=op)
     stress, strain, info = b.homogenize()
     inf = mb.info_array(info)
     assert (inf["status"] == 0).all(), inf
@@ -76,14 +78,16 @@ def test_same_result_alone_and_in_mix():
     assert np.array_equal(s_again, s_mix)
 
 
-@pytest.mark.parametrize("threads,ctas,cluster", [(512, 1, 1), (512, 2, 1), (256, 2, 1),
-                                                   (256, 4, 1), (512, 2, 2), (512, 1, 4),
-                                                   (512, 2, 8)])
-def test_cta_shapes_agree(threads, ctas, cluster):
+@pytest.mark.parametrize("threads,ctas,cluster,op", [
+    (512, 1, 1, mb.SP_OP_ELL), (512, 2, 1, mb.SP_OP_ELL), (256, 2, 1, mb.SP_OP_ELL),
+    (256, 4, 1, mb.SP_OP_ELL), (512, 2, 2, mb.SP_OP_ELL), (512, 1, 4, mb.SP_OP_ELL),
+    (512, 2, 8, mb.SP_OP_ELL), (512, 1, 1, mb.SP_OP_STENCIL), (512, 2, 1, mb.SP_OP_STENCIL),
+    (256, 2, 1, mb.SP_OP_STENCIL), (256, 4, 1, mb.SP_OP_STENCIL)])
+def test_cta_shapes_agree(threads, ctas, cluster, op):
     """Every CTA shape, and RVEs split over thread-block clusters of 2, 4
     and 8 CTAs, give the oracle's result."""
     descs = make_descs(9, [5, 3, 6, 2, 8, 12])
-    b = mb.Batch(descs, threads=threads, ctas_per_sm=ctas, cluster=cluster)
+    b = mb.Batch(descs, threads=threads, ctas_per_sm=ctas, cluster=cluster, op=op)
     s, _, info = b.homogenize()
     assert (mb.info_array(info)["status"] == 0).all()
     for i, d in enumerate(descs):
@@ -93,8 +97,28 @@ def test_cta_shapes_agree(threads, ctas, cluster):
 
 def test_cluster_result_is_deterministic():
     descs = make_descs(21, [6, 10, 4])
-    a, _, _ = mb.Batch(descs, cluster=4).homogenize()
-    b, _, _ = mb.Batch(descs, cluster=4).homogenize()
-    c, _, _ = mb.Batch(descs[1:2], cluster=4).homogenize()
+    a, _, _ = mb.Batch(descs, cluster=4, op=mb.SP_OP_ELL).homogenize()
+    b, _, _ = mb.Batch(descs, cluster=4, op=mb.SP_OP_ELL).homogenize()
+    c, _, _ = mb.Batch(descs[1:2], cluster=4, op=mb.SP_OP_ELL).homogenize()
     assert np.array_equal(a, b)
     assert np.array_equal(a[1], c[0])
+
+
+def test_stencil_and_assembled_agree_on_boxes():
+    """Non-cubic meshes (nx != ny != nz, unequal edge lengths): the stencil
+    operator and the assembled ELL operator reach the same tangent."""
+    descs = make_descs(5, [4, 6, 5, 3])
+    for d, n, ln in zip(descs, [(3, 5, 4), (6, 2, 7), (5, 5, 9), (2, 3, 2)],
+                        [(1.0, 1.5, 0.8), (2.0, 1.0, 1.0), (1.0, 1.0, 1.7), (0.5, 1.0, 1.0)]):
+        d.n[0], d.n[1], d.n[2] = n
+        d.len[0], d.len[1], d.len[2] = ln
+    a, _, ia = mb.Batch(descs, op=mb.SP_OP_STENCIL).homogenize()
+    b, _, ib = mb.Batch(descs, op=mb.SP_OP_ELL).homogenize()
+    assert (mb.info_array(ia)["status"] == 0).all() and (mb.info_array(ib)["status"] == 0).all()
+    for i in range(len(descs)):
+        assert np.abs(a[i] - b[i]).max() <= 2e-8 * np.abs(b[i]).max(), i
+
+
+def test_unknown_batch_option_is_rejected():
+    with pytest.raises(TypeError):
+        mb.batch_opts(oprator=1)
