@@ -58,22 +58,28 @@ def nnz_true(n: int) -> int:
     return 9 * (3 * (n + 1) - 2) ** 3
 
 
-def algorithmic_bytes(sizes, inner_its, outer_its, k=6):
-    """Bytes the batched solve must move per launch: per CG iteration the
-    FP32 matrix values (4 B per structural nonzero) plus one int32 column
-    node per 3x3 block (the node-sliced ELL stores one per block), the SpMM
-    input/output vectors and 8 FP32 vector passes; per refinement step 3 FP64
-    vector passes; the assembly writes once."""
+def algorithmic_bytes(sizes, inner_its, outer_its, k=6, stencil=True):
+    """Bytes the batched solve must move per launch.  Per CG iteration: the
+    SpMM input and output vectors, plus, for the assembled operator, the
+    FP32 matrix values (4 B per structural nonzero) and one int32 column node
+    per 3x3 block (the node-sliced ELL stores one per block), or, for the
+    stencil operator, one material byte per element; and 8 FP32 vector
+    passes.  Per refinement step 3 FP64 vector passes.  Once per RVE the
+    assembled values (written) or the stencil's Jacobi diagonal."""
     total = 0.0
     for n, it, ot in zip(sizes, inner_its, outer_its):
         n, it, ot = int(n), float(it), float(ot)
         ndof = 3 * (n + 1) ** 3
         nelm = n ** 3
-        spmm = nnz_true(n) * 4 + nnz_true(n) // 9 * 4 + 2 * k * ndof * 4
+        if stencil:
+            spmm = nelm + 2 * k * ndof * 4
+            setup = ndof * 4
+        else:
+            spmm = nnz_true(n) * 4 + nnz_true(n) // 9 * 4 + 2 * k * ndof * 4
+            setup = nelm * (576 * 4 + 24 * 4)
         vec = 8 * k * ndof * 4
         refine = 3 * k * ndof * 8
-        assemble = nelm * (576 * 4 + 24 * 4)
-        total += it * (spmm + vec) + (ot + 1) * refine + assemble
+        total += it * (spmm + vec) + (ot + 1) * refine + setup
     return total
 
 
@@ -237,7 +243,8 @@ def run_ours(args):
     sizes = [d.n[0] for d in descs]
     t0 = time.time()
     batch = mb.Batch(descs, nrhs=6, threads=args.threads, ctas_per_sm=args.ctas,
-                     cluster=args.cluster, inner_rtol=args.inner_rtol)
+                     cluster=args.cluster, inner_rtol=args.inner_rtol,
+                     op=mb.SP_OP_STENCIL if args.op == "stencil" else mb.SP_OP_ELL)
     setup_s = time.time() - t0
 
     for _ in range(args.warmup):
@@ -305,7 +312,7 @@ def run_ours(args):
 
     line = None
     if rank == 0:
-        abytes = algorithmic_bytes(sizes, inf["inner"], inf["outer"])
+        abytes = algorithmic_bytes(sizes, inf["inner"], inf["outer"], stencil=args.op == "stencil")
         avg_ms = total_ms / args.steps
         achieved = abytes / (avg_ms / 1000.0) / 1e9
         peak, peak_kind = measured_peak()
@@ -319,6 +326,7 @@ def run_ours(args):
                        "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8,
                        "precision": "mixed", "cta_threads": args.threads, "ctas_per_sm": args.ctas,
                        "cluster": args.cluster, "inner_rtol": args.inner_rtol,
+                       "operator": args.op,
                        "l2": "inputs larger than L2 (FP32 ELL values alone are "
                              f"{sum(3 * (n + 1) ** 3 * 84 * 4 for n in sizes) / 1e9:.1f} GB)",
                        "parallelism": f"replicas x{world} (independent RVEs per rank)"},
@@ -464,6 +472,8 @@ def main(argv=None):
     ap.add_argument("--ctas", type=int, default=2)
     ap.add_argument("--cluster", type=int, default=1)
     ap.add_argument("--inner-rtol", type=float, default=1e-4)
+    ap.add_argument("--op", default="stencil", choices=["stencil", "ell"],
+                    help="inner CG operator: element-type stencil or assembled ELL values")
     ap.add_argument("--sizes", type=int, nargs="+", default=list(SIZES),
                     help="mesh sizes to draw from (the headline workload uses 8 12 16 20)")
     ap.add_argument("--e2e-steps", type=int, default=3)

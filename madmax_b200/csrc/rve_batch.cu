@@ -126,10 +126,12 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: nrhs must be 1..%d", SP_MAX_RHS);
   if (o.precision != SP_PREC_MIXED && o.precision != SP_PREC_FP64)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown precision");
-  // CTA shape: 512 threads x 1 or 2 CTAs per SM, or 256 threads x 2 or 4
+  // CTA shape: 512 threads x 1 or 2 CTAs per SM, 256 threads x 2 or 4, or
+  // (stencil operator) 1024 threads x 1
   if (o.threads == 0) o.threads = 512;
-  if (o.threads != 256 && o.threads != 512)
-    return sp_set_error(SP_ERR_ARG, "sp_batch_create: threads must be 256 or 512");
+  if (o.threads != 256 && o.threads != 512 && o.threads != 1024)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: threads must be 256, 512 or 1024");
+  if (o.threads == 1024) o.ctas_per_sm = 1;
   if (o.ctas_per_sm == 0) o.ctas_per_sm = 2;
   if (o.threads == 512 && o.ctas_per_sm != 1 && o.ctas_per_sm != 2)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: 512-thread CTAs run 1 or 2 per SM");

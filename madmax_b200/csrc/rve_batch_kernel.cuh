@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   constexpr bool STENCIL = OP == SP_OP_STENCIL;
   __shared__ double sKe[2 * SP_KE];
   // element scatter values (assembled operator) or element blocks (stencil)
-  __shared__ __align__(16) T sKeT[STENCIL ? 2 * SP_KB_TYPE : 2 * SP_KE];
+  __shared__ __align__(16) T sKeT[STENCIL ? SP_KB_SIZE : 2 * SP_KE];
   __shared__ double sD[72], sBbar[144], sdsh[192];
   // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
   __shared__ double red[33 * 16];
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     __syncthreads();
     T *nsv = nullptr, *dinv;
     if constexpr (STENCIL) {
-      // 2s. no assembly: the 3x3 element blocks and the Jacobi diagonal
+      // 2s. no assembly: the stencil block tables and the Jacobi diagonal
       dinv = reinterpret_cast<T *>(P.ws_dinv) + (size_t)slot * P.drm_stride;
       stencil_blocks<T>(t, NT, sKe, sKeT);
       stencil_dinv<T>(gt, GNT, g, etype, sKe, dinv);
@@ -171,7 +171,8 @@ using BatchFn = void (*)(BatchParams);
   X(T, K, 512, 1, 4, SP_OP_ELL) X(T, K, 512, 2, 4, SP_OP_ELL) X(T, K, 512, 1, 8, SP_OP_ELL) \
   X(T, K, 512, 2, 8, SP_OP_ELL) \
   X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL) \
-  X(T, K, 256, 2, 1, SP_OP_STENCIL) X(T, K, 256, 4, 1, SP_OP_STENCIL)
+  X(T, K, 256, 2, 1, SP_OP_STENCIL) X(T, K, 256, 4, 1, SP_OP_STENCIL) \
+  X(T, K, 1024, 1, 1, SP_OP_STENCIL)
 #define SP_BATCH_SHAPES_FP64(X, T, K) \
   X(T, K, 512, 1, 1, SP_OP_ELL) X(T, K, 512, 2, 1, SP_OP_ELL) \
   X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL)

@@ -649,16 +649,41 @@ __host__ __device__ constexpr int hex8_local(int cx, int cy, int cz) {
   return cz * 4 + (cy == 0 ? (cx ? 1 : 0) : (cx ? 2 : 3));
 }
 
-constexpr int SP_KB_BLK = 12;                 // padded 3x3 block (16-byte rows for float)
-constexpr int SP_KB_TYPE = 64 * SP_KB_BLK;    // blocks of one material
+constexpr int SP_KB_BLK = 12;                        // padded 3x3 block (16-byte rows for float)
+constexpr int SP_KB_TYPE = 64 * SP_KB_BLK;           // element blocks of one material
+constexpr int SP_KA_OFF = 0;                         // KA[t][m]: 2 x 27 blocks
+constexpr int SP_KE_OFF = 2 * 27 * SP_KB_BLK;        // KE[t][la][lb]: 2 x 64 blocks
+constexpr int SP_KB_SIZE = SP_KE_OFF + 2 * SP_KB_TYPE;
 
-// KB[ty][(la*8 + lb)*12 + 3d + c] = Ke[ty][3la + d][3lb + c] in T, pads 0
+// Shared tables of the stencil operator (T values, summed in FP64 and
+// rounded once; block entry 3d + c, 3 zero pads):
+//   KA[t][m]      the assembled block of neighbour m = (dx+1) + 3(dy+1) + 9(dz+1)
+//                 of a node whose 8 elements are all of material t;
+//   KE[t][la][lb] Ke[t][3la + d][3lb + c], the element blocks.
 template <typename T>
 __device__ inline void stencil_blocks(int t, int nt, const double *Ke /*[2][576]*/, T *KB) {
-  for (int x = t; x < 2 * SP_KB_TYPE; x += nt) {
-    int ty = x / SP_KB_TYPE, r = x % SP_KB_TYPE, b = r / SP_KB_BLK, w = r % SP_KB_BLK;
-    int la = b / 8, lb = b % 8;
-    KB[x] = (w < 9) ? (T)Ke[ty * SP_KE + (3 * la + w / 3) * SP_NC + 3 * lb + w % 3] : T(0);
+  for (int x = t; x < SP_KB_SIZE; x += nt) {
+    double v = 0.0;
+    const int w = x % SP_KB_BLK;
+    if (w < 9) {
+      const int d = w / 3, cc = w % 3;
+      if (x < SP_KE_OFF) {
+        const int ty = x / (27 * SP_KB_BLK), m = (x / SP_KB_BLK) % 27;
+        const int dx = m % 3 - 1, dy = (m / 3) % 3 - 1, dz = m / 9 - 1;
+        for (int c = 0; c < 8; c++) {
+          const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+          const int bx = 1 - ox + dx, by = 1 - oy + dy, bz = 1 - oz + dz;
+          if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+          const int la = hex8_local(1 - ox, 1 - oy, 1 - oz), lb = hex8_local(bx, by, bz);
+          v += Ke[ty * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
+        }
+      } else {
+        const int r = x - SP_KE_OFF, ty = r / SP_KB_TYPE, b = (r % SP_KB_TYPE) / SP_KB_BLK;
+        const int la = b / 8, lb = b % 8;
+        v = Ke[ty * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
+      }
+    }
+    KB[x] = (T)v;
   }
 }
 
@@ -686,16 +711,93 @@ __device__ inline void stencil_dinv(int t, int nt, const MeshGeo &g,
   }
 }
 
+// 3x3 block load from shared memory (16-byte loads), accumulated into bv
+template <typename T, typename A>
+__device__ inline void add_block(const T *src, A *bv) {
+  constexpr int BW = SP_KB_BLK * (int)sizeof(T) / 16;
+  T w[SP_KB_BLK];
+#pragma unroll
+  for (int q = 0; q < BW; q++) {
+    int4 v = reinterpret_cast<const int4 *>(src)[q];
+    memcpy(reinterpret_cast<char *>(w) + 16 * q, &v, 16);
+  }
+#pragma unroll
+  for (int u = 0; u < 9; u++) bv[u] += (A)w[u];
+}
+
+// Accumulators of the stencil SpMM: FP32 pairs of load cases updated with
+// the packed FP32x2 FMA, or FP64 scalars.
+template <typename T, int K>
+struct StencilAcc;
+
+template <int K>
+struct StencilAcc<float, K> {
+  static constexpr int KP = (K + 1) / 2;
+  float2 v[3][KP];
+  __device__ void zero() {
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int p = 0; p < KP; p++) v[d][p] = make_float2(0.f, 0.f);
+  }
+  // v[d][q] += bv(d, c) x[q][c][nb]
+  __device__ void fma_block(const float *bv, const float *x, size_t blk, int nn_pad, int nb) {
+#pragma unroll
+    for (int p = 0; p < KP; p++) {
+      float2 xb[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        xb[c].x = x[(2 * p) * blk + (size_t)c * nn_pad + nb];
+        xb[c].y = (2 * p + 1 < K) ? x[(2 * p + 1) * blk + (size_t)c * nn_pad + nb] : 0.f;
+      }
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          const float b = bv[d * 3 + c];
+          v[d][p] = __ffma2_rn(make_float2(b, b), xb[c], v[d][p]);
+        }
+    }
+  }
+  __device__ float get(int d, int q) const { return (q & 1) ? v[d][q >> 1].y : v[d][q >> 1].x; }
+};
+
+template <int K>
+struct StencilAcc<double, K> {
+  double v[3][K];
+  __device__ void zero() {
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int q = 0; q < K; q++) v[d][q] = 0.0;
+  }
+  __device__ void fma_block(const double *bv, const double *x, size_t blk, int nn_pad, int nb) {
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      double xb[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) xb[c] = x[q * blk + (size_t)c * nn_pad + nb];
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[d][q] = fma(bv[d * 3 + c], xb[c], v[d][q]);
+    }
+  }
+  __device__ double get(int d, int q) const { return v[d][q]; }
+};
+
 // y = A x (K right-hand sides, component-major) with the stencil operator on
 // interior nodes; boundary and padding entries of y are not written.  A warp
-// takes 32 consecutive interior nodes (x fastest), a lane one node.  Adds
-// x.y per load case into dot[K].
+// takes 32 consecutive interior nodes (x fastest), a lane one node.  A warp
+// whose nodes all lie inside one material reads that material's assembled
+// blocks (one shared-memory broadcast per load); other warps sum each
+// neighbour block from the element blocks of their own materials.  Adds x.y
+// per load case into dot[K].
 template <typename T, int K>
 __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB,
                                     const uint8_t *__restrict__ etype, const T *x, T *y,
                                     double *dot) {
   using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
-  constexpr int BW = SP_KB_BLK * (int)sizeof(T) / 16;  // 16-byte words per block
   const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
   const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
   const int ni = mx * my * mz;
@@ -709,55 +811,52 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
     const int a = i + j * sy + k * sz;
     const int e0 = (i - 1) + (j - 1) * esy + (k - 1) * esz;
     int tb[8];  // offset of the element's material blocks in KB
+    unsigned mask = 0;
 #pragma unroll
-    for (int c = 0; c < 8; c++)
-      tb[c] = (int)__ldg(etype + e0 + (c & 1) + ((c >> 1) & 1) * esy + (c >> 2) * esz) *
-              SP_KB_TYPE;
-    A acc[3][K];
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-#pragma unroll
-      for (int q = 0; q < K; q++) acc[d][q] = A(0);
-    // neighbour planes dz = -1, 0, 1 in turn (a rolled loop bounds the live
-    // registers); within a plane the 9 neighbours and their elements unroll
+    for (int c = 0; c < 8; c++) {
+      const unsigned te = __ldg(etype + e0 + (c & 1) + ((c >> 1) & 1) * esy + (c >> 2) * esz);
+      mask |= te << c;
+      tb[c] = SP_KE_OFF + (int)te * SP_KB_TYPE;
+    }
+    StencilAcc<T, K> acc;
+    acc.zero();
+    const bool all0 = __all_sync(0xffffffffu, mask == 0u);
+    const bool all1 = __all_sync(0xffffffffu, mask == 0xffu);
+    if (all0 || all1) {
+      // one material around every node of the warp: its assembled blocks
+      const T *ka = KB + SP_KA_OFF + (all1 ? 27 * SP_KB_BLK : 0);
 #pragma unroll 1
-    for (int dz = -1; dz <= 1; dz++) {
+      for (int dz = -1; dz <= 1; dz++) {
 #pragma unroll
-      for (int m = 0; m < 9; m++) {
-        const int dx = m % 3 - 1, dy = m / 3 - 1;
-        A bv[9];
-#pragma unroll
-        for (int w = 0; w < 9; w++) bv[w] = A(0);
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-          const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
-          const int bx = 1 - ox + dx, by = 1 - oy + dy;
-          if (bx < 0 || bx > 1 || by < 0 || by > 1) continue;  // resolved at compile time
-          const int bz = 1 - oz + dz;                            // warp-uniform
-          if (bz < 0 || bz > 1) continue;
-          const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
-          const int lb = hex8_local(bx, by, 0) + 4 * bz;
-          const int4 *src =
-              reinterpret_cast<const int4 *>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK);
-          T w[SP_KB_BLK];
-#pragma unroll
-          for (int q = 0; q < BW; q++) {
-            int4 v = src[q];
-            memcpy(reinterpret_cast<char *>(w) + 16 * q, &v, 16);
-          }
-#pragma unroll
-          for (int u = 0; u < 9; u++) bv[u] += (A)w[u];
+        for (int mm = 0; mm < 9; mm++) {
+          const int dx = mm % 3 - 1, dy = mm / 3 - 1;
+          A bv[9] = {};
+          add_block<T, A>(ka + ((dz + 1) * 9 + mm) * SP_KB_BLK, bv);
+          acc.fma_block(bv, x, blk, g.nn_pad, a + dx + dy * sy + dz * sz);
         }
-        const int nb = a + dx + dy * sy + dz * sz;
+      }
+    } else {
+      // neighbour planes dz = -1, 0, 1 in turn (a rolled loop bounds the
+      // live registers); within a plane the 9 neighbours and their elements
+      // unroll
+#pragma unroll 1
+      for (int dz = -1; dz <= 1; dz++) {
 #pragma unroll
-        for (int q = 0; q < K; q++) {
-          A xb[3];
+        for (int mm = 0; mm < 9; mm++) {
+          const int dx = mm % 3 - 1, dy = mm / 3 - 1;
+          A bv[9] = {};
 #pragma unroll
-          for (int c = 0; c < 3; c++) xb[c] = (A)x[q * blk + (size_t)c * g.nn_pad + nb];
-#pragma unroll
-          for (int d = 0; d < 3; d++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) acc[d][q] = fma(bv[d * 3 + c], xb[c], acc[d][q]);
+          for (int c = 0; c < 8; c++) {
+            const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+            const int bx = 1 - ox + dx, by = 1 - oy + dy;
+            if (bx < 0 || bx > 1 || by < 0 || by > 1) continue;  // resolved at compile time
+            const int bz = 1 - oz + dz;                            // warp-uniform
+            if (bz < 0 || bz > 1) continue;
+            const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+            const int lb = hex8_local(bx, by, 0) + 4 * bz;
+            add_block<T, A>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK, bv);
+          }
+          acc.fma_block(bv, x, blk, g.nn_pad, a + dx + dy * sy + dz * sz);
         }
       }
     }
@@ -767,7 +866,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           size_t o = q * blk + (size_t)d * g.nn_pad + a;
-          T yv = (T)acc[d][q];
+          T yv = (T)acc.get(d, q);
           dot[q] += (double)yv * (double)x[o];
           y[o] = yv;
         }
