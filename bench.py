@@ -83,6 +83,102 @@ def algorithmic_bytes(sizes, inner_its, outer_its, k=6, stencil=True):
     return total
 
 
+def l2_note(args, sizes, batch):
+    if args.op == "ell":
+        return ("inputs larger than L2 (FP32 ELL values alone are "
+                f"{sum(3 * (n + 1) ** 3 * 84 * 4 for n in sizes) / 1e9:.1f} GB)")
+    return ("inputs larger than L2: the stencil keeps no matrix; the batch's device buffers "
+            f"(CG work spaces of the RVEs in flight, plans, materials) are "
+            f"{batch.device_bytes() / 1e9:.2f} GB")
+
+
+def structured_ell(n: int, seed: int = 5):
+    """84-slot ELL with the sparsity of the hex8 RVE stiffness on an n^3 mesh:
+    row 3a + d holds the 3 dofs of every node within one grid step of node a
+    (stored slots first, -1 after), random values."""
+    N = n + 1
+    nn = N ** 3
+    a = np.arange(nn, dtype=np.int64)
+    i, j, k = a % N, (a // N) % N, a // (N * N)
+    nbs = []
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                ok = ((i + dx >= 0) & (i + dx < N) & (j + dy >= 0) & (j + dy < N) &
+                      (k + dz >= 0) & (k + dz < N))
+                nbs.append(np.where(ok, a + dx + dy * N + dz * N * N, -1))
+    nb = np.stack(nbs, 1)
+    cols = np.where(nb[:, :, None] >= 0, 3 * nb[:, :, None] + np.arange(3), -1).reshape(nn, 81)
+    cols = np.take_along_axis(cols, np.argsort(cols < 0, axis=1, kind="stable"), 1)
+    full = np.full((3 * nn, 84), -1, np.int32)
+    full[:, :81] = np.repeat(cols, 3, axis=0)
+    vals = np.where(full >= 0, np.random.default_rng(seed).uniform(-1.0, 1.0, full.shape), 0.0)
+    return full, vals
+
+
+def measure_spmv(mb, stream, sptr, n=40, reps=20):
+    """The resident FP64 ELL SpMV (sp_ell_dev_mvp) on one matrix larger than
+    L2, L2 flushed before every launch, at every lanes-per-row setting;
+    achieved = algorithmic bytes (stored slots x 12 + x read + y write) /
+    CUDA-event time per launch."""
+    import torch
+    cols, vals = structured_ell(n)
+    m = mb.ell_matrix()
+    m.nrow = m.ncol = cols.shape[0]
+    m.nnz = cols.shape[1]
+    m.cols = cols.ctypes.data_as(C.POINTER(C.c_int))
+    m.vals = vals.ctypes.data_as(C.POINTER(C.c_double))
+    h = mb._vp()
+    mb.check(mb.lib().sp_ell_upload(C.byref(m), C.byref(h)), "sp_ell_upload")
+    try:
+        nrow, wp, nnz = C.c_int(), C.c_int(), C.c_longlong()
+        mb.check(mb.lib().sp_ell_dev_info(h, C.byref(nrow), C.byref(wp), C.byref(nnz)), "info")
+        x_h = np.random.default_rng(6).standard_normal(nrow.value)
+        x = torch.from_numpy(x_h).cuda()
+        y = torch.empty_like(x)
+        xp, yp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())
+        # spot check of 2000 rows against numpy
+        mb.check(mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr), "mvp")
+        torch.cuda.synchronize()
+        rows = np.arange(0, nrow.value, max(1, nrow.value // 2000))
+        cr = cols[rows]
+        ref = (vals[rows] * np.where(cr >= 0, x_h[np.maximum(cr, 0)], 0.0)).sum(1)
+        err = float(np.abs(y.cpu().numpy()[rows] - ref).max() / np.abs(ref).max())
+        # every timed launch starts from a cold L2: a 256 MB buffer (> 126 MB
+        # L2) is rewritten before it, outside the events
+        flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+        per = {}
+        for lanes in (4, 8, 16, 32):
+            mb.check(mb.lib().sp_ell_dev_set_lanes(h, lanes), "lanes")
+            for _ in range(3):
+                mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr)
+            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(reps)]
+            torch.cuda.synchronize()
+            for e0, e1 in evs:
+                flush.fill_(1.0)
+                e0.record(stream)
+                mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            per[lanes] = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
+        del flush
+        best = min(per, key=per.get)
+        abytes = nnz.value * 12 + 2 * nrow.value * 8
+        peak, peak_kind = measured_peak()
+        ach = abytes / (per[best] / 1e3) / 1e9
+        return {"kernel": "k_spmv_rve (sp_ell_dev_mvp, FP64 ELL, hoisted loads)",
+                "matrix": f"hex8 RVE sparsity n={n}: {nrow.value} rows x 84 slots, "
+                          f"{nnz.value} stored, {(vals.nbytes + cols.nbytes) / 1e6:.0f} MB > L2",
+                "l2": "flushed before every timed launch",
+                "lanes_per_row": best, "ms": per[best],
+                "ms_by_lanes": {str(k): round(v, 4) for k, v in per.items()},
+                "algorithmic_bytes": abytes, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_kind": peak_kind, "max_rel_err_vs_numpy": err}
+    finally:
+        mb.lib().sp_ell_dev_free(h)
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -327,8 +423,7 @@ def run_ours(args):
                        "precision": "mixed", "cta_threads": args.threads, "ctas_per_sm": args.ctas,
                        "cluster": args.cluster, "inner_rtol": args.inner_rtol,
                        "operator": args.op,
-                       "l2": "inputs larger than L2 (FP32 ELL values alone are "
-                             f"{sum(3 * (n + 1) ** 3 * 84 * 4 for n in sizes) / 1e9:.1f} GB)",
+                       "l2": l2_note(args, sizes, batch),
                        "parallelism": f"replicas x{world} (independent RVEs per rank)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
@@ -342,6 +437,8 @@ def run_ours(args):
                       "mean_outer_its": float(inf["outer"].mean()),
                       "rhs_solves_per_s": 6 * value, "setup_s": setup_s},
         }
+        if world == 1 and not args.no_spmv:
+            line["spmv"] = measure_spmv(mb, stream, sptr)
         if world == 1 and not args.no_plain:
             line["plain_gpu"] = plain_gpu(mb, descs, args)
             line["plain_gpu"]["batched_speedup"] = value / line["plain_gpu"]["value"]
@@ -482,6 +579,7 @@ def main(argv=None):
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--serve-geoms", type=int, default=256)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[1e3, 1e4, 1e5])
     ap.add_argument("--serve-seconds", type=float, default=2.0)

@@ -72,6 +72,12 @@ int sp_ell_dev_free(sp_ell_dev *a);
 int sp_ell_dev_mvp(sp_ell_dev *a, const double *x_dev, double *y_dev, void *stream);
 /* Same with host vectors (copies in and out). */
 int sp_ell_dev_mvp_host(sp_ell_dev *a, const double *x, double *y);
+/* Lanes per row of sp_ell_dev_mvp: 4, 8, 16 or 32 (0: the library's choice,
+ * 8 for 84-slot rows).  A tuning knob; the result does not depend on it
+ * beyond rounding. */
+int sp_ell_dev_set_lanes(sp_ell_dev *a, int lanes);
+/* Rows, padded row width and stored (non-empty) slots of a device matrix. */
+int sp_ell_dev_info(const sp_ell_dev *a, int *nrow, int *wp, long long *true_nnz);
 /* Jacobi-preconditioned CG in FP64 on host vectors: the ELL path of the
  * reference's solve() (micro/src/homogenize.c:320-333) with PETSc's
  * KSPCG + PCJACOBI algorithm; stops at ||b - A x|| <= rtol ||b||.  x holds
@@ -216,15 +222,17 @@ typedef struct {
   double rtol;          /* default 1e-8 */
   double inner_rtol;    /* default 1e-4 */
   int idle_spin_limit;  /* empty polls before the loop returns (0: default) */
-  int pad;
+  int op;               /* SP_OP_STENCIL (default) or SP_OP_ELL */
+  int ctas_per_sm;      /* request slots per SM: 1 or 2 (0: 1 for the stencil, 2 for ELL) */
 } sp_server_opts;
 
 void sp_server_opts_default(sp_server_opts *o);
 
 typedef struct sp_server_s sp_server;
-/* Makes every geometry resident (assembled FP32 ELL, FP64 element
- * operators, warm-start store) while the running total stays within the
- * budget; returns SP_ERR_BUDGET, creating nothing, if it does not. */
+/* Makes every geometry resident (FP64 element operators, Jacobi diagonal,
+ * warm-start store, and for SP_OP_ELL the assembled FP32 ELL values) while
+ * the running total stays within the budget; returns SP_ERR_BUDGET,
+ * creating nothing, if it does not. */
 int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_server_opts *o,
                      sp_server **out);
 int sp_server_destroy(sp_server *s);

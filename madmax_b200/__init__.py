@@ -71,7 +71,7 @@ class sp_batch_opts(C.Structure):
 class sp_server_opts(C.Structure):
     _fields_ = [("hbm_budget", C.c_size_t), ("max_inflight", C.c_int),
                 ("queue_capacity", C.c_int), ("rtol", C.c_double), ("inner_rtol", C.c_double),
-                ("idle_spin_limit", C.c_int), ("pad", C.c_int)]
+                ("idle_spin_limit", C.c_int), ("op", C.c_int), ("ctas_per_sm", C.c_int)]
 
 
 # ------------------------------------------------------------------- loader ---
@@ -110,6 +110,8 @@ _PROTOS = {
     "sp_ell_dev_free": (C.c_int, [_vp]),
     "sp_ell_dev_mvp": (C.c_int, [_vp, _vp, _vp, _vp]),
     "sp_ell_dev_mvp_host": (C.c_int, [_vp, _dp, _dp]),
+    "sp_ell_dev_set_lanes": (C.c_int, [_vp, C.c_int]),
+    "sp_ell_dev_info": (C.c_int, [_vp, _ip, _ip, C.POINTER(C.c_longlong)]),
     "sp_ell_dev_pcg": (C.c_int, [_vp, _dp, _dp, C.c_double, C.c_int, _ip, _dp]),
     "sp_ell_pcg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_double, C.c_int,
                                      _ip, _dp, _vp]),
@@ -402,7 +404,10 @@ def info_array(info) -> np.ndarray:
 def server_opts(**kw) -> sp_server_opts:
     o = sp_server_opts()
     lib().sp_server_opts_default(C.byref(o))
+    names = {f[0] for f in sp_server_opts._fields_}
     for k, v in kw.items():
+        if k not in names:
+            raise TypeError(f"unknown server option {k!r}")
         setattr(o, k, v)
     return o
 

@@ -135,6 +135,17 @@ struct Scratch {
 static std::mutex g_ell_mu;
 static Scratch g_ell_scratch[64];
 
+// y = A x on the 84-slot RVE layout, L lanes per row: every lane issues all
+// its value and column loads before its gathers (spmm_rve).
+template <int L>
+__global__ void __launch_bounds__(PCG_THREADS) k_spmv_rve(int n, const double *__restrict__ vals,
+                                                          const int *__restrict__ cols,
+                                                          const double *__restrict__ x, double *y) {
+  double dummy[1] = {0.0};
+  spmm_rve<double, 1, L, true>(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, n,
+                               vals, cols, x, y, dummy);
+}
+
 static int launch_blocks(Device *d, long long warps_needed) {
   long long b = (warps_needed + 7) / 8;
   long long cap = (long long)d->nsm * 8;
@@ -291,6 +302,8 @@ extern "C" int ell_solve_jacobi(ell_solver *solver, ell_matrix *m, double *b, do
 
 struct sp_ell_dev_s {
   int nrow, ncol, nnz, wp, dev;
+  int lanes = 0;  // lanes per row of the SpMV (0: chosen by the library)
+  long long true_nnz = 0;  // stored (non-empty) slots
   int *cols = nullptr;    // [nrow][wp]
   double *vals = nullptr; // [nrow][wp]
   double *dinv = nullptr;
@@ -331,6 +344,7 @@ extern "C" int sp_ell_upload(const ell_matrix *m, sp_ell_dev **out) {
         hc[(size_t)r * a->wp + j] = c;
         hv[(size_t)r * a->wp + j] = (c >= 0) ? m->vals[(size_t)r * m->nnz + j] : 0.0;
         if (c == r) diag = hv[(size_t)r * a->wp + j];
+        if (c >= 0) a->true_nnz++;
       }
       hd[r] = 1.0 / diag;
     }
@@ -377,10 +391,38 @@ extern "C" int sp_ell_dev_mvp(sp_ell_dev *a, const double *x_dev, double *y_dev,
   Device *d;
   SP_TRY(device(&d));
   cudaStream_t s = pick_stream(stream, d);
-  int nb = launch_blocks(d, a->nrow);
-  k_spmm_plain<double, 1, 32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->wp, a->vals, a->cols, x_dev,
-                                                         y_dev);
+  if (a->wp == SP_WP) {
+    // RVE-shaped rows: 84 slots, loads hoisted; 8 lanes (4 rows per warp) by default
+    const int L = a->lanes ? a->lanes : 8;
+    int nb = launch_blocks(d, ((long long)a->nrow * L + 31) / 32);
+    switch (L) {
+      case 4: k_spmv_rve<4><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
+      case 8: k_spmv_rve<8><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
+      case 16: k_spmv_rve<16><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
+      default: k_spmv_rve<32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
+    }
+  } else {
+    int nb = launch_blocks(d, a->nrow);
+    k_spmm_plain<double, 1, 32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->wp, a->vals, a->cols,
+                                                           x_dev, y_dev);
+  }
   SP_CUDA_TRY(cudaGetLastError());
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_set_lanes(sp_ell_dev *a, int lanes) {
+  if (!a) return sp_set_error(SP_ERR_ARG, "sp_ell_dev_set_lanes: null matrix");
+  if (lanes != 0 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
+    return sp_set_error(SP_ERR_ARG, "sp_ell_dev_set_lanes: lanes must be 0, 4, 8, 16 or 32");
+  a->lanes = lanes;
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_info(const sp_ell_dev *a, int *nrow, int *wp, long long *true_nnz) {
+  if (!a) return sp_set_error(SP_ERR_ARG, "sp_ell_dev_info: null matrix");
+  if (nrow) *nrow = a->nrow;
+  if (wp) *wp = a->wp;
+  if (true_nnz) *true_nnz = a->true_nnz;
   return SP_OK;
 }
 

@@ -14,9 +14,10 @@
 //     into a device ring and publishes the device count;
 //   - every other CTA is a worker slot: it claims the next published request
 //     (atomic counter), solves it with the same per-RVE solve as the batched
-//     kernel (rve_solve.cuh) on the geometry's resident FP32 ELL matrix,
-//     warm-started from that geometry's previous solution, writes the result
-//     to mapped memory and raises the request's done flag.
+//     kernel (rve_solve.cuh) -- on the element-type stencil (default) or on
+//     the geometry's resident FP32 ELL matrix -- warm-started from that
+//     geometry's previous solution, writes the result to mapped memory and
+//     raises the request's done flag.
 // A request is picked up as soon as any slot is free, while other requests
 // are still solving: their work overlaps on the device.  Every wait is
 // bounded (idle_spin_limit polls); on expiry the CTA returns and the host
@@ -44,7 +45,7 @@ struct ServeGeom {
   MeshGeo g;
   const int *cols;
   const int *nbr;
-  float *vals;  // node-sliced ELL values [nn_pad*243]
+  float *vals;  // node-sliced ELL values [nn_pad*243] (assembled operator only)
   float *dinv;  // component-major [3][nn_pad]
   const uint8_t *etype;
   double *Ke;   // [2][576]
@@ -98,10 +99,12 @@ struct ServeParams {
   int max_outer, max_inner, idle_limit;
 };
 
-// Assemble every geometry once (a CTA takes geometries in turn): element
-// operators kept in global memory, FP32 ELL values by the coloured scatter
-// into the CTA's row-major scratch, Dirichlet rows/columns, then the
-// node-sliced copy the solve reads.
+// Prepare every geometry once (a CTA takes geometries in turn): element
+// operators kept in global memory and the Jacobi diagonal; for the assembled
+// operator also the FP32 ELL values by the coloured scatter into the CTA's
+// row-major scratch, Dirichlet rows/columns, then the node-sliced copy the
+// solve reads.
+template <int OP>
 __global__ void __launch_bounds__(SERVE_NT) k_serve_assemble(ServeGeom *geoms, int ngeom,
                                                              const double *mats, float *scratch,
                                                              size_t rm_stride, size_t drm_stride) {
@@ -125,6 +128,11 @@ __global__ void __launch_bounds__(SERVE_NT) k_serve_assemble(ServeGeom *geoms, i
     }
     for (int i = t; i < 72; i += SERVE_NT) G.D[i] = sD[i];
     for (int i = t; i < 144; i += SERVE_NT) G.Bbar[i] = sB[i];
+    if constexpr (OP == SP_OP_STENCIL) {
+      stencil_dinv<float>(t, SERVE_NT, g, G.etype, sKe, G.dinv);
+      __syncthreads();
+      continue;
+    }
     ell_zero<float>(t, SERVE_NT, vrm, g.ndof);
     __syncthreads();
     for (int c = 0; c < 8; c++) {
@@ -140,8 +148,11 @@ __global__ void __launch_bounds__(SERVE_NT) k_serve_assemble(ServeGeom *geoms, i
   }
 }
 
-__global__ void __launch_bounds__(SERVE_NT, 2) k_serve(ServeParams P) {
+template <int OP, int MINB>
+__global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
+  constexpr bool STENCIL = OP == SP_OP_STENCIL;
   __shared__ double sKe[2 * SP_KE], sD[72], sB[144];
+  __shared__ __align__(16) float sKB[STENCIL ? SP_KB_SIZE : 4];
   __shared__ double red[33 * 16];
   __shared__ double savg[SP_MAX_RHS * 12];
   __shared__ double seps[SERVE_K * 6];
@@ -255,6 +266,7 @@ __global__ void __launch_bounds__(SERVE_NT, 2) k_serve(ServeParams P) {
     if (warm)
       for (size_t i = t; i < nu; i += SERVE_NT) u[i] = __ldcg(G.warm + i);
     __syncthreads();
+    if constexpr (STENCIL) stencil_blocks<float>(t, SERVE_NT, sKe, sKB);
     affine_soa<SERVE_K>(t, SERVE_NT, g, seps, SERVE_NRHS, warm, u);
     __syncthreads();
     SolveArgs sa;
@@ -263,9 +275,16 @@ __global__ void __launch_bounds__(SERVE_NT, 2) k_serve(ServeParams P) {
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
-    EllOp<float, SERVE_K> op{G.vals, G.nbr};
-    sp_solve_info in = solve_rve<float, SERVE_K, SERVE_NT, 1>(
-        g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p, q, sa, red, &sh, savg);
+    sp_solve_info in;
+    if constexpr (STENCIL) {
+      StencilOp<float, SERVE_K> op{sKB, G.etype};
+      in = solve_rve<float, SERVE_K, SERVE_NT, 1>(g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p,
+                                                  q, sa, red, &sh, savg);
+    } else {
+      EllOp<float, SERVE_K> op{G.vals, G.nbr};
+      in = solve_rve<float, SERVE_K, SERVE_NT, 1>(g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p,
+                                                  q, sa, red, &sh, savg);
+    }
     // keep this solution as the geometry's next warm start
     for (size_t i = t; i < nu; i += SERVE_NT) __stcg(G.warm + i, u[i]);
     __threadfence();
@@ -293,11 +312,13 @@ static double now_s() {
   return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
-static size_t geom_bytes(const sp_rve_desc &d) {
+// device bytes a resident geometry holds (the assembled operator adds its
+// node-sliced FP32 values)
+static size_t geom_bytes(const sp_rve_desc &d, int op) {
   size_t nn = (size_t)(d.n[0] + 1) * (d.n[1] + 1) * (d.n[2] + 1), np = (nn + 31) / 32 * 32;
   size_t nelm = (size_t)d.n[0] * d.n[1] * d.n[2];
-  return np * 243 * 4 + 3 * np * 4 + nelm + (2 * SP_KE + 72 + 144) * 8 + SERVE_K * 3 * np * 8 +
-         1024;
+  return (op == SP_OP_ELL ? np * 243 * 4 : 0) + 3 * np * 4 + nelm +
+         (2 * SP_KE + 72 + 144) * 8 + SERVE_K * 3 * np * 8 + 1024;
 }
 
 }  // namespace sp
@@ -325,6 +346,13 @@ struct sp_server_s {
 
 static int server_grid(sp_server *s, Device *d);
 
+// the loop kernel for an operator and a CTAs-per-SM target
+using ServeFn = void (*)(ServeParams);
+static ServeFn serve_kernel(const sp_server_opts &o) {
+  if (o.op == SP_OP_ELL) return o.ctas_per_sm == 1 ? k_serve<SP_OP_ELL, 1> : k_serve<SP_OP_ELL, 2>;
+  return o.ctas_per_sm == 1 ? k_serve<SP_OP_STENCIL, 1> : k_serve<SP_OP_STENCIL, 2>;
+}
+
 extern "C" void sp_server_opts_default(sp_server_opts *o) {
   memset(o, 0, sizeof(*o));
   o->hbm_budget = (size_t)150 * 1000 * 1000 * 1000;
@@ -333,6 +361,8 @@ extern "C" void sp_server_opts_default(sp_server_opts *o) {
   o->rtol = 1e-8;
   o->inner_rtol = 1e-4;
   o->idle_spin_limit = 2000000;
+  o->op = SP_OP_STENCIL;
+  o->ctas_per_sm = 0;
 }
 
 static int server_layout(int ngeom, const sp_rve_desc *descs, const sp_server_opts *o, int nsm,
@@ -345,7 +375,7 @@ static int server_layout(int ngeom, const sp_rve_desc *descs, const sp_server_op
     for (int k = 0; k < 3; k++)
       if (d.n[k] < 1 || d.len[k] <= 0)
         return sp_set_error(SP_ERR_ARG, "geometry %d: bad mesh", i);
-    resident += geom_bytes(d);
+    resident += geom_bytes(d, o->op);
     std::vector<int> key(d.n, d.n + 3);
     if (!seen.count(key)) {
       seen[key] = 1;
@@ -354,7 +384,8 @@ static int server_layout(int ngeom, const sp_rve_desc *descs, const sp_server_op
     maxnp = std::max(maxnp, ((d.n[0] + 1) * (d.n[1] + 1) * (d.n[2] + 1) + 31) / 32 * 32);
   }
   size_t slot = (size_t)SERVE_K * 3 * maxnp * (8 + 4 * 4);
-  int want = nsm * 2 - 1;
+  const int per_sm = o->ctas_per_sm ? o->ctas_per_sm : (o->op == SP_OP_STENCIL ? 1 : 2);
+  int want = nsm * per_sm - 1;
   if (o->max_inflight > 0 && o->max_inflight < want) want = o->max_inflight;
   size_t budget = o->hbm_budget ? o->hbm_budget : (size_t)150e9;
   if (resident + slot > budget)
@@ -406,6 +437,12 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   if (!(o.rtol > 0)) o.rtol = 1e-8;
   if (!(o.inner_rtol > 0)) o.inner_rtol = 1e-4;
   if (o.idle_spin_limit <= 0) o.idle_spin_limit = 2000000;
+  if (o.op != SP_OP_ELL && o.op != SP_OP_STENCIL)
+    return sp_set_error(SP_ERR_ARG, "sp_server_create: unknown operator");
+  // the stencil solve of 7 load cases wants 128 registers (1 slot per SM)
+  if (o.ctas_per_sm == 0) o.ctas_per_sm = (o.op == SP_OP_STENCIL) ? 1 : 2;
+  if (o.ctas_per_sm != 1 && o.ctas_per_sm != 2)
+    return sp_set_error(SP_ERR_ARG, "sp_server_create: ctas_per_sm must be 1 or 2");
   Device *d;
   SP_TRY(device(&d));
   int slots;
@@ -446,10 +483,11 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
     maxdof = std::max(maxdof, G.g.ndof);
     maxnp = std::max(maxnp, G.g.nn_pad);
     size_t np = G.g.nn_pad, ne = G.g.nelm;
-    void *b[7];
-    size_t sz[7] = {np * 243 * 4, 3 * np * 4, ne + 16, 2 * SP_KE * 8, 72 * 8, 144 * 8,
-                    SERVE_K * 3 * np * 8};
+    void *b[7] = {};
+    size_t sz[7] = {o.op == SP_OP_ELL ? np * 243 * 4 : 0, 3 * np * 4, ne + 16, 2 * SP_KE * 8,
+                    72 * 8, 144 * 8, SERVE_K * 3 * np * 8};
     for (int k = 0; k < 7 && !rc; k++) {
+      if (!sz[k]) continue;
       rc = dmalloc(&b[k], sz[k], &s->bytes);
       if (!rc) s->dbufs.push_back(b[k]);
     }
@@ -477,7 +515,8 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   int nasm = std::min(ngeom, 2 * d->nsm);
   if (!rc) rc = dmalloc((void **)&s->d_geoms, ngeom * sizeof(ServeGeom), &s->bytes);
   if (!rc) rc = dmalloc((void **)&d_mats, mats.size() * sizeof(double), nullptr);
-  if (!rc) rc = dmalloc((void **)&d_scr, (size_t)nasm * (rm_stride + drm_stride) * 4, nullptr);
+  if (!rc && o.op == SP_OP_ELL)
+    rc = dmalloc((void **)&d_scr, (size_t)nasm * (rm_stride + drm_stride) * 4, nullptr);
   if (!rc) rc = dmalloc((void **)&s->d_req, (size_t)s->cap * sizeof(ServeReq), &s->bytes);
   if (!rc) rc = dmalloc((void **)&s->d_dev, sizeof(ServeDev), &s->bytes);
   if (!rc) rc = dmalloc((void **)&s->ws_u, (size_t)s->grid * s->stride * 8, &s->bytes);
@@ -501,8 +540,12 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
       rc = sp_set_error(SP_ERR_CUDA, "server upload");
   }
   if (!rc) {
-    k_serve_assemble<<<nasm, SERVE_NT, 0, s->stream>>>(s->d_geoms, ngeom, d_mats, d_scr, rm_stride,
-                                                      drm_stride);
+    if (o.op == SP_OP_STENCIL)
+      k_serve_assemble<SP_OP_STENCIL><<<nasm, SERVE_NT, 0, s->stream>>>(
+          s->d_geoms, ngeom, d_mats, d_scr, rm_stride, drm_stride);
+    else
+      k_serve_assemble<SP_OP_ELL><<<nasm, SERVE_NT, 0, s->stream>>>(
+          s->d_geoms, ngeom, d_mats, d_scr, rm_stride, drm_stride);
     if (cudaGetLastError() || cudaStreamSynchronize(s->stream))
       rc = sp_set_error(SP_ERR_CUDA, "geometry assembly failed");
   }
@@ -537,7 +580,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
 // dispatcher's counter): the grid never exceeds what the SMs hold.
 static int server_grid(sp_server *s, Device *d) {
   int occ = 0;
-  SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_serve, SERVE_NT, 0));
+  SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, serve_kernel(s->o), SERVE_NT, 0));
   if (occ < 1) return sp_set_error(SP_ERR_CUDA, "serving kernel does not fit an SM");
   int cap = d->nsm * occ;
   if (s->grid > cap) s->grid = cap;
@@ -552,7 +595,7 @@ static int server_launch(sp_server *s) {
   z.dispatcher_gone = 0;
   SP_CUDA_TRY(cudaMemcpyAsync(s->d_dev, &z, sizeof(z), cudaMemcpyHostToDevice, s->stream));
   SP_CUDA_TRY(cudaStreamSynchronize(s->stream));
-  k_serve<<<s->grid, SERVE_NT, 0, s->stream>>>(s->P);
+  serve_kernel(s->o)<<<s->grid, SERVE_NT, 0, s->stream>>>(s->P);
   SP_CUDA_TRY(cudaGetLastError());
   s->running = 1;
   return SP_OK;

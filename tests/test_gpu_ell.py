@@ -111,6 +111,32 @@ def test_ell_dev_mvp_and_pcg():
         mb.lib().sp_ell_dev_free(h)
 
 
+@pytest.mark.parametrize("lanes", [0, 4, 8, 16, 32])
+def test_ell_dev_mvp_every_lane_width(lanes):
+    """The resident SpMV at every lanes-per-row setting matches the
+    reference-order product within rounding; true_nnz counts stored slots."""
+    m = O.cube_mesh(6)
+    et = O.fiber_types(m, [1, 1], 0.25)
+    A = O.assemble(m, et, (1e9, 3e10), (0.3, 0.2), symmetric_bc=True)
+    B = as_lib_matrix(A.cols.copy(), A.vals.copy())
+    h = mb._vp()
+    mb.check(mb.lib().sp_ell_upload(C.byref(B.m), C.byref(h)), "upload")
+    try:
+        mb.check(mb.lib().sp_ell_dev_set_lanes(h, lanes), "lanes")
+        nrow, wp, nnz = C.c_int(), C.c_int(), C.c_longlong()
+        mb.check(mb.lib().sp_ell_dev_info(h, C.byref(nrow), C.byref(wp), C.byref(nnz)), "info")
+        assert nrow.value == m.ndof and wp.value == 84
+        assert nnz.value == int((A.cols >= 0).sum())
+        x = np.random.default_rng(lanes).standard_normal(m.ndof)
+        y = np.zeros(m.ndof)
+        mb.check(mb.lib().sp_ell_dev_mvp_host(h, mb.ptr(x), mb.ptr(y)), "mvp")
+        yo = A.mvp(x)
+        assert np.abs(y - yo).max() <= 1e-13 * np.abs(yo).max()
+        assert mb.lib().sp_ell_dev_set_lanes(h, 3) == mb.SP_ERR_ARG
+    finally:
+        mb.lib().sp_ell_dev_free(h)
+
+
 def test_reference_unity_program_linked_to_library(golden_dir, tmp_path):
     """The reference's unity/unity_ell.c, compiled unchanged against
     include/ell.h and linked to libsputnik_b200.so (oracle/Makefile target

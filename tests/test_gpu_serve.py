@@ -31,9 +31,10 @@ def oracle_fd(d, eps):
     return s0, Cm
 
 
-def test_serve_matches_oracle():
+@pytest.mark.parametrize("op", [mb.SP_OP_STENCIL, mb.SP_OP_ELL])
+def test_serve_matches_oracle(op):
     G = geoms()
-    s = mb.Server(G)
+    s = mb.Server(G, op=op)
     s.start()
     rng = np.random.default_rng(1)
     reqs = [(int(rng.integers(0, len(G))), rng.normal(0, 1e-3, 6)) for _ in range(12)]
