@@ -444,6 +444,8 @@ def run_ours(args):
             line["plain_gpu"]["batched_speedup"] = value / line["plain_gpu"]["value"]
         if world == 1 and not args.no_serve:
             line["serving"] = serving(mb, args)
+        if world == 1 and not args.no_fe2:
+            line["fe2"] = fe2_step(mb, args)
         if world == 1 and not args.no_cpu:
             per, wall, res = cpu_sample(args.cpu_sample, 77, 1)
             line["cpu_baseline"] = {
@@ -469,6 +471,44 @@ def serve_geometries(mb, ngeom: int, seed: int):
     nu_f = rng.uniform(0.2, 0.35, size=ngeom)
     return [mb.rve_desc(int(n[i]), float(radius[i]), (E_MATRIX, E_MATRIX * float(ratio[i])),
                         (float(nu_m[i]), float(nu_f[i]))) for i in range(ngeom)]
+
+
+def fe2_step(mb, args):
+    """A full FE2 step: 40x10x10 hex8 cantilever (14,883 dof, 32,000 Gauss
+    points), tip traction 1e6 Pa, every Gauss point bound to one of 64
+    seeded RVEs (n = 16, fibre radius U(0.15, 0.3), matrix E 1e9 nu 0.3,
+    fibre E 1e10 nu 0.2), 5 Newton iterations, FP64 macro solve; the micro
+    tangents come from the serving loop."""
+    rng = np.random.default_rng(5150)
+    rves = [mb.rve_desc(16, float(rng.uniform(0.15, 0.3)), (1e9, 1e10), (0.3, 0.2))
+            for _ in range(64)]
+    t0 = time.perf_counter()
+    f = mb.Fe2(rves, newton_its=5)
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    info = f.run()
+    step = time.perf_counter() - t0
+    f.close()
+    out = {"macro": "40x10x10 hex8 cantilever, 14883 dof, 32000 Gauss points, traction 1e6 Pa",
+           "rves": "64 x n=16 (seeded)", "micro": "linear: FD tangent around zero per RVE",
+           "micro_setup_s": setup, "step_s": step, "newton_its": info.newton_its,
+           "bnorm": [info.bnorm[i] for i in range(info.newton_its)],
+           "pcg_its": [info.pcg_its[i] for i in range(info.newton_its)],
+           "tip_displacement": list(info.tip), "micro_requests": info.micro_requests,
+           "device_ms": {"residual": info.residual_ms, "assemble": info.assemble_ms,
+                         "solve": info.solve_ms}}
+    if args.fe2_per_gp:
+        # iteration 1 sees zero strains everywhere (answered from the warm
+        # starts); iteration 2 solves 32,000 distinct strains
+        t0 = time.perf_counter()
+        g = mb.Fe2(rves, newton_its=2, micro=mb.SP_FE2_PER_GP)
+        gi = g.run()
+        out["per_gauss_point"] = {"newton_its": 2, "requests": gi.micro_requests,
+                                  "micro_s": gi.micro_s, "total_s": time.perf_counter() - t0,
+                                  "requests_per_s": gi.micro_requests / gi.micro_s,
+                                  "tip_displacement": list(gi.tip)}
+        g.close()
+    return out
 
 
 def serving(mb, args):
@@ -580,6 +620,9 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
+    ap.add_argument("--no-fe2", action="store_true")
+    ap.add_argument("--fe2-per-gp", action="store_true",
+                    help="also time one Newton iteration with a serving request per Gauss point")
     ap.add_argument("--serve-geoms", type=int, default=256)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[1e3, 1e4, 1e5])
     ap.add_argument("--serve-seconds", type=float, default=2.0)

@@ -259,6 +259,65 @@ int sp_server_replay(sp_server *s, int nreq, const int *geom, const double *stra
                      const double *t_arrival, double *t_done, double *stress, double *tangent,
                      sp_solve_info *info, double timeout_s);
 
+/* -------------------------------------------------------------------- FE2 */
+
+/* An FE2 step on one GPU: the macro Newton loop of macro/src/main.c:202-256
+ * (residual macro/src/assembly.c:5-84, Jacobian :165-222, clamped rows and
+ * columns :208-214) on a structured hex8 cantilever of n[0] x n[1] x n[2]
+ * elements, clamped at x = 0 and loaded by a uniform traction on x = len[0];
+ * every macro Gauss point takes its stress and tangent from one of nrve
+ * micro RVEs served by sp_server.  FP64 macro assembly and Jacobi-PCG. */
+#define SP_FE2_LINEAR 0 /* linear micro materials: one FD tangent around zero strain
+                           per RVE (micro/src/init.c:54-59), then sigma = C eps
+                           (micro/src/homogenize.c:3-21) */
+#define SP_FE2_PER_GP 1 /* one serving-loop request (stress + FD tangent) per Gauss
+                           point per Newton iteration */
+#define SP_FE2_MAX_ITS 16
+
+typedef struct {
+  int n[3];              /* macro elements per axis (default 40 x 10 x 10) */
+  double len[3];         /* macro box edges (default 4 x 1 x 1) */
+  double traction[3];    /* Pa on the face x = len[0] (default (0, 0, -1e6)) */
+  int nrve;              /* micro RVEs */
+  const sp_rve_desc *rves;
+  const int *gp_rve;     /* [nelm*8] RVE of each Gauss point (element-major), NULL: seeded */
+  int newton_its;        /* Newton iterations, 1..SP_FE2_MAX_ITS (default 5) */
+  double newton_tol;     /* stop once ||b|| <= tol (default 0: all iterations) */
+  double lin_rtol;       /* macro PCG relative tolerance (default 1e-10) */
+  double strain_clip;    /* |eps_v| below this is set to 0 (reference: 1e-6,
+                            macro/src/assembly.c:319) */
+  int micro;             /* SP_FE2_LINEAR (default) or SP_FE2_PER_GP */
+  int seed;              /* seed of the Gauss point -> RVE binding when gp_rve is NULL */
+} sp_fe2_desc;
+
+void sp_fe2_desc_default(sp_fe2_desc *d);
+
+typedef struct {
+  int newton_its;                 /* iterations run */
+  int pcg_its[SP_FE2_MAX_ITS];    /* macro PCG iterations per Newton iteration */
+  double bnorm[SP_FE2_MAX_ITS];   /* ||b|| at the start of each Newton iteration */
+  double tip[3];                  /* mean displacement of the loaded face */
+  long long micro_requests;       /* serving-loop requests made */
+  double micro_s, macro_s;        /* wall time in micro requests / the macro loop */
+  double residual_ms, assemble_ms, solve_ms; /* device time (CUDA events), summed over
+                                                iterations: strains + stresses + residual,
+                                                Jacobian assembly, PCG + update */
+} sp_fe2_info;
+
+typedef struct sp_fe2_s sp_fe2;
+/* Builds the macro problem, starts a serving loop over the RVEs and, for
+ * SP_FE2_LINEAR, obtains every RVE's tangent around zero strain. */
+int sp_fe2_create(const sp_fe2_desc *d, sp_fe2 **out);
+/* Runs the Newton loop from u = 0. */
+int sp_fe2_run(sp_fe2 *f, sp_fe2_info *info);
+/* Macro displacement, [3 * (n0+1) * (n1+1) * (n2+1)], node = i + nx (j + ny k). */
+int sp_fe2_displacement(const sp_fe2 *f, double *u);
+/* The Gauss point -> RVE binding, [nelm*8]. */
+int sp_fe2_gp_rve(const sp_fe2 *f, int *gp_rve);
+/* SP_FE2_LINEAR: the RVE tangents used, [nrve][36] row-major. */
+int sp_fe2_micro_tangents(const sp_fe2 *f, double *C);
+int sp_fe2_destroy(sp_fe2 *f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,23 @@ class sp_server_opts(C.Structure):
                 ("idle_spin_limit", C.c_int), ("op", C.c_int), ("ctas_per_sm", C.c_int)]
 
 
+SP_FE2_LINEAR, SP_FE2_PER_GP, SP_FE2_MAX_ITS = 0, 1, 16
+
+
+class sp_fe2_desc(C.Structure):
+    _fields_ = [("n", C.c_int * 3), ("len", C.c_double * 3), ("traction", C.c_double * 3),
+                ("nrve", C.c_int), ("rves", C.POINTER(sp_rve_desc)), ("gp_rve", C.POINTER(C.c_int)),
+                ("newton_its", C.c_int), ("newton_tol", C.c_double), ("lin_rtol", C.c_double),
+                ("strain_clip", C.c_double), ("micro", C.c_int), ("seed", C.c_int)]
+
+
+class sp_fe2_info(C.Structure):
+    _fields_ = [("newton_its", C.c_int), ("pcg_its", C.c_int * 16), ("bnorm", C.c_double * 16),
+                ("tip", C.c_double * 3), ("micro_requests", C.c_longlong),
+                ("micro_s", C.c_double), ("macro_s", C.c_double), ("residual_ms", C.c_double),
+                ("assemble_ms", C.c_double), ("solve_ms", C.c_double)]
+
+
 # ------------------------------------------------------------------- loader ---
 
 # name -> (restype, argtypes); every symbol the public headers declare
@@ -116,6 +133,13 @@ _PROTOS = {
     "sp_ell_pcg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_double, C.c_int,
                                      _ip, _dp, _vp]),
     "sp_classify": (C.c_int, [C.POINTER(sp_rve_desc), _up]),
+    "sp_fe2_desc_default": (None, [C.POINTER(sp_fe2_desc)]),
+    "sp_fe2_create": (C.c_int, [C.POINTER(sp_fe2_desc), C.POINTER(_vp)]),
+    "sp_fe2_run": (C.c_int, [_vp, C.POINTER(sp_fe2_info)]),
+    "sp_fe2_displacement": (C.c_int, [_vp, _dp]),
+    "sp_fe2_gp_rve": (C.c_int, [_vp, _ip]),
+    "sp_fe2_micro_tangents": (C.c_int, [_vp, _dp]),
+    "sp_fe2_destroy": (C.c_int, [_vp]),
     "sp_ell_pattern": (C.c_int, [_ip, _ip]),
     "sp_rve_create": (C.c_int, [C.POINTER(sp_rve_desc), C.POINTER(_vp)]),
     "sp_rve_destroy": (C.c_int, [_vp]),
@@ -473,6 +497,68 @@ class Server:
     def close(self):
         if self.h:
             lib().sp_server_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------- FE2
+
+class Fe2:
+    """FE2 cantilever step (sp_fe2_*): macro Newton loop on the GPU, micro
+    RVEs through the serving loop."""
+
+    def __init__(self, rves, gp_rve=None, **kw):
+        self.d = sp_fe2_desc()
+        lib().sp_fe2_desc_default(C.byref(self.d))
+        names = {f[0] for f in sp_fe2_desc._fields_}
+        for k, v in kw.items():
+            if k not in names or k in ("rves", "gp_rve", "nrve"):
+                raise TypeError(f"unknown FE2 option {k!r}")
+            if k in ("n", "len", "traction"):
+                getattr(self.d, k)[:] = v
+            else:
+                setattr(self.d, k, v)
+        self._rves = (sp_rve_desc * len(rves))(*rves)
+        self.d.nrve = len(rves)
+        self.d.rves = self._rves
+        self._gp = None
+        if gp_rve is not None:
+            self._gp = np.ascontiguousarray(gp_rve, dtype=np.int32)
+            self.d.gp_rve = self._gp.ctypes.data_as(C.POINTER(C.c_int))
+        self.h = _vp()
+        check(lib().sp_fe2_create(C.byref(self.d), C.byref(self.h)), "sp_fe2_create")
+        n = list(self.d.n)
+        self.ndof = 3 * (n[0] + 1) * (n[1] + 1) * (n[2] + 1)
+        self.ngp = 8 * n[0] * n[1] * n[2]
+
+    def run(self) -> sp_fe2_info:
+        info = sp_fe2_info()
+        check(lib().sp_fe2_run(self.h, C.byref(info)), "sp_fe2_run")
+        return info
+
+    def displacement(self) -> np.ndarray:
+        u = np.zeros(self.ndof)
+        check(lib().sp_fe2_displacement(self.h, ptr(u)), "sp_fe2_displacement")
+        return u
+
+    def gp_rve(self) -> np.ndarray:
+        g = np.zeros(self.ngp, dtype=np.int32)
+        check(lib().sp_fe2_gp_rve(self.h, ptr(g, _ip)), "sp_fe2_gp_rve")
+        return g
+
+    def micro_tangents(self) -> np.ndarray:
+        Cm = np.zeros((self.d.nrve, 6, 6))
+        check(lib().sp_fe2_micro_tangents(self.h, ptr(Cm)), "sp_fe2_micro_tangents")
+        return Cm
+
+    def close(self):
+        if self.h:
+            lib().sp_fe2_destroy(self.h)
             self.h = _vp()
 
     def __del__(self):

@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
+    sa.warm = 0;
     sp_solve_info in;
     if constexpr (STENCIL) {
       StencilOp<T, K> op{sKeT, etype};

@@ -875,8 +875,10 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 }
 
 // b = -K u on interior dofs, 0 on the boundary and on padding (component-
-// major vectors; see residual_nodes for the arithmetic).
-template <int K, typename R>
+// major vectors; see residual_nodes for the arithmetic).  BCONLY: u's
+// interior values are read as 0, giving the right-hand side -K u_bc of the
+// load cases.
+template <int K, typename R, bool BCONLY = false>
 __device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
                                     const uint8_t *__restrict__ etype,
                                     const double *Ke /*[2][576], shared*/,
@@ -903,6 +905,7 @@ __device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
 #pragma unroll 2
           for (int b = 0; b < 8; b++) {
             int nb = n0 + corner_x(b) + corner_y(b) * g.nx + corner_z(b) * g.nx * g.ny;
+            if (BCONLY && !is_bnode(g, nb)) continue;
 #pragma unroll
             for (int db = 0; db < 3; db++) {
               double kv = ke[b * 3 + db];

@@ -28,6 +28,7 @@ struct SolveArgs {
   int nrhs;
   double rtol, inner_rtol;
   int max_outer, max_inner;
+  int warm;  // u's interior holds a start iterate other than 0
 };
 
 struct CgShared {
@@ -165,6 +166,25 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
   if (t == 0) sh->phase = 0;
   int outer = 0, inner = 0;
   rve_sync<CL>();
+  if (P.warm) {
+    // The stopping rule is relative to the right-hand side, the residual of
+    // the boundary values alone (not to the residual of the start iterate,
+    // which a good warm start makes tiny).  A load case whose right-hand
+    // side vanishes has the solution 0 inside.
+    double m0[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) m0[k] = 0.0;
+    residual_soa<K, T, true>(gt, GNT, g, etype, sKe, u, r, m0);
+    rve_reduce<K, CL>(m0, red, sh);
+    if (warp == 0 && lane < K) sh->rn0[lane] = sqrt(red[32 * K + lane]);
+    __syncthreads();
+    for (int k = 0; k < P.nrhs; k++) {
+      if (sh->rn0[k] > 0.0) continue;
+      for (int idx = gt; idx < blk; idx += GNT)
+        if (idx % g.nn_pad < g.nn && !is_bnode(g, idx % g.nn_pad)) u[(size_t)k * blk + idx] = 0.0;
+    }
+    rve_sync<CL>();
+  }
   for (;;) {
     // 3a. FP64 residual b = -K u -> r (type T) and its norms
     {
@@ -177,7 +197,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         bool notdone = false;
         if (lane < K) {
           double rn = sqrt(red[32 * K + lane]);
-          if (outer == 0) sh->rn0[lane] = rn;
+          if (outer == 0 && !P.warm) sh->rn0[lane] = rn;
           sh->rn[lane] = rn;
           double rn0 = sh->rn0[lane];
           notdone = lane < P.nrhs && rn0 > 0.0 && rn > P.rtol * rn0;

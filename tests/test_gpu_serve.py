@@ -106,3 +106,28 @@ def test_budget_refusal_and_bad_geometry():
     assert mb.lib().sp_server_submit(s.h, len(G), mb.ptr(e), C.byref(t)) == mb.SP_ERR_RANGE
     s.stop()
     s.close()
+
+
+def test_repeated_and_zero_strain_requests_converge():
+    """A warm start that already solves the request (the same strain again)
+    stops at once, and a zero strain (zero right-hand side of the base load
+    case) is answered with zero stress: the stopping rule is relative to the
+    right-hand side, not to the warm start's residual."""
+    G = geoms()
+    s = mb.Server(G)
+    s.start()
+    e = np.array([2e-4, -1e-4, 3e-4, 0.0, 1e-4, -2e-4])
+    st1, tg1, i1 = s.wait(s.submit(2, e))
+    st2, tg2, i2 = s.wait(s.submit(2, e))
+    z = np.zeros(6)
+    st0, tg0, i0 = s.wait(s.submit(2, z))
+    st0b, tg0b, i0b = s.wait(s.submit(2, z))
+    s.stop()
+    s.close()
+    for i in (i1, i2, i0, i0b):
+        assert i.status == 0 and i.relres <= 1e-8
+    assert i2.inner_its < i1.inner_its
+    assert np.abs(st2 - st1).max() <= 2e-8 * np.abs(st1).max()
+    assert np.abs(st0).max() <= 1e-9 * np.abs(st1).max()
+    assert np.abs(tg0 - tg1).max() <= 1e-7 * np.abs(tg1).max()
+    assert np.abs(tg0b - tg1).max() <= 1e-7 * np.abs(tg1).max()
