@@ -162,6 +162,11 @@ int sp_rve_tangent(sp_rve *r, double rtol, double *C, sp_solve_info *info);
 #define SP_PREC_MIXED 0 /* FP32 ELL values + FP32 CG, FP64 residual refinement */
 #define SP_PREC_FP64 1  /* FP64 values and CG */
 
+#define SP_BC_AFFINE 0   /* u = eps.x on every boundary node (micro/src/homogenize.c:227-242) */
+#define SP_BC_PERIODIC 1 /* u = eps.x + w, w periodic, corners at eps.x: the master-slave form
+                            (BC_PER_MS, micro/inc/micro.h:26) of the reference's 2D periodic
+                            conditions (micro/src/assembly.c:175-220, 272-354), in 3D */
+
 #define SP_OP_ELL 0     /* inner CG on the RVE's assembled ELL values (coloured scatter) */
 #define SP_OP_STENCIL 1 /* inner CG on the element-type stencil: A p from the two element
                            stiffnesses and the element materials, no matrix in memory */
@@ -178,6 +183,7 @@ typedef struct {
   int ctas_per_sm;   /* resident CTAs per SM: 1 or 2 (512 threads), 2 or 4 (256) */
   int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 (assembled) */
   int op;            /* SP_OP_STENCIL (default) or SP_OP_ELL */
+  int bc;            /* SP_BC_AFFINE (default) or SP_BC_PERIODIC (stencil only) */
 } sp_batch_opts;
 
 void sp_batch_opts_default(sp_batch_opts *o);

@@ -22,6 +22,7 @@ ELL_ERR_CUDA = 5
 SP_ID_MATRIX, SP_ID_FIBER = 0, 1
 SP_PREC_MIXED, SP_PREC_FP64 = 0, 1
 SP_OP_ELL, SP_OP_STENCIL = 0, 1
+SP_BC_AFFINE, SP_BC_PERIODIC = 0, 1
 SP_MAX_RHS = 8
 SP_NOALLOC_MAX_ROWS = 262144
 MAX_ITS, MIN_ERR = 100000, 1.0e-10
@@ -65,7 +66,7 @@ class sp_batch_opts(C.Structure):
     _fields_ = [("nrhs", C.c_int), ("precision", C.c_int), ("rtol", C.c_double),
                 ("inner_rtol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
                 ("threads", C.c_int), ("lanes_per_row", C.c_int), ("ctas_per_sm", C.c_int),
-                ("cluster", C.c_int), ("op", C.c_int)]
+                ("cluster", C.c_int), ("op", C.c_int), ("bc", C.c_int)]
 
 
 class sp_server_opts(C.Structure):

@@ -69,6 +69,8 @@ MeshGeo make_geo(const int *n, const double *len) {
   g.hy = len[1] / n[1];
   g.hz = len[2] / n[2];
   g.vol = len[0] * len[1] * len[2];
+  g.periodic = 0;
+  g.pad = 0;
   return g;
 }
 

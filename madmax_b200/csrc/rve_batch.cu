@@ -66,6 +66,11 @@ static BatchFn pick(int prec, int K, const Shape &s) {
 
 static int kpad(int nrhs) { return nrhs == 1 ? 1 : (nrhs <= 6 ? 6 : 8); }
 
+// the kernel variant of an operator and boundary condition
+static int kernel_op(const sp_batch_opts &o) {
+  return (o.op == SP_OP_STENCIL && o.bc == SP_BC_PERIODIC) ? SP_OP_STENCIL_PER : o.op;
+}
+
 }  // namespace sp
 
 using namespace sp;
@@ -101,6 +106,7 @@ extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   o->ctas_per_sm = 2;
   o->cluster = 1;
   o->op = SP_OP_STENCIL;
+  o->bc = SP_BC_AFFINE;
 }
 
 extern "C" int sp_batch_destroy(sp_batch *b) {
@@ -143,14 +149,23 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: cluster must be 1, 2, 4 or 8");
   if (o.op != SP_OP_ELL && o.op != SP_OP_STENCIL)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown operator");
+  if (o.bc != SP_BC_AFFINE && o.bc != SP_BC_PERIODIC)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown boundary condition");
+  if (o.bc == SP_BC_PERIODIC && o.op != SP_OP_STENCIL)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: periodic conditions need the stencil operator");
+  if (o.bc == SP_BC_PERIODIC && (o.cluster != 1 || o.threads != 512))
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: periodic conditions run 512-thread CTAs, no cluster");
   if (o.max_outer < 1) o.max_outer = 8;
   if (o.max_inner < 1) o.max_inner = 4000;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
   if (!(o.inner_rtol > 0)) o.inner_rtol = 1e-4;
   for (int i = 0; i < nrve; i++)
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k < 3; k++) {
       if (descs[i].n[k] < 1 || descs[i].len[k] <= 0)
         return sp_set_error(SP_ERR_ARG, "sp_batch_create: RVE %d has a bad mesh", i);
+      if (o.bc == SP_BC_PERIODIC && descs[i].n[k] < 2)
+        return sp_set_error(SP_ERR_ARG, "sp_batch_create: periodic RVE %d needs 2 elements per axis", i);
+    }
   Device *d;
   SP_TRY(device(&d));
   sp_batch *b = new sp_batch_s();
@@ -215,7 +230,7 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   int nrhs = o.nrhs, kp = b->kp;
   // persistent grid: as many clusters as can be resident at once
   {
-    Shape sh{o.threads, o.ctas_per_sm, o.cluster, o.op};
+    Shape sh{o.threads, o.ctas_per_sm, o.cluster, kernel_op(o)};
     BatchFn fn = pick(o.precision, kp, sh);
     if (!fn && !rc)
       rc = sp_set_error(SP_ERR_ARG, "sp_batch_create: no kernel for %d threads x %d CTAs/SM, "
@@ -350,7 +365,7 @@ extern "C" int sp_batch_launch(sp_batch *b, void *stream) {
   Device *d;
   SP_TRY(device(&d));
   cudaStream_t s = pick_stream(stream, d);
-  Shape sh{b->o.threads, b->o.ctas_per_sm, b->o.cluster, b->o.op};
+  Shape sh{b->o.threads, b->o.ctas_per_sm, b->o.cluster, kernel_op(b->o)};
   BatchFn fn = pick(b->o.precision, b->nrhs, sh);
   SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
   if (b->o.cluster == 1) {

@@ -8,6 +8,10 @@
 
 namespace sp {
 
+// kernel operator variants: SP_OP_ELL, SP_OP_STENCIL, and the stencil under
+// periodic boundary conditions
+constexpr int SP_OP_STENCIL_PER = 2;
+
 struct BatchPlan {
   MeshGeo geo; // node/element counts; h and vol per RVE
   const int *cols;
@@ -51,7 +55,8 @@ struct BatchParams {
 
 template <typename T, int K, int NT, int MINB, int CL, int OP>
 __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
-  constexpr bool STENCIL = OP == SP_OP_STENCIL;
+  constexpr bool PER = OP == SP_OP_STENCIL_PER;
+  constexpr bool STENCIL = OP == SP_OP_STENCIL || PER;
   __shared__ double sKe[2 * SP_KE];
   // element scatter values (assembled operator) or element blocks (stencil)
   __shared__ __align__(16) T sKeT[STENCIL ? SP_KB_SIZE : 2 * SP_KE];
@@ -60,6 +65,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   __shared__ double red[33 * 16];
   __shared__ double savg[SP_MAX_RHS * 12];
   __shared__ CgShared sh;
+  __shared__ double seps[SP_MAX_RHS * 6];
   __shared__ int s_job;
   const int t = threadIdx.x;
   const int rank = rve_rank<CL>();
@@ -95,6 +101,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     g.hy = rv.len[1] / g.ney;
     g.hz = rv.len[2] / g.nez;
     g.vol = rv.len[0] * rv.len[1] * rv.len[2];
+    g.periodic = PER ? 1 : 0;
     const uint8_t *etype = P.etype + rv.etype_off;
 
     // 1. element operators (every CTA keeps its own copy)
@@ -109,7 +116,10 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
       // 2s. no assembly: the stencil block tables and the Jacobi diagonal
       dinv = reinterpret_cast<T *>(P.ws_dinv) + (size_t)slot * P.drm_stride;
       stencil_blocks<T>(t, NT, sKe, sKeT);
-      stencil_dinv<T>(gt, GNT, g, etype, sKe, dinv);
+      if constexpr (PER)
+        stencil_dinv_per<T>(gt, GNT, g, etype, sKe, dinv);
+      else
+        stencil_dinv<T>(gt, GNT, g, etype, sKe, dinv);
     } else {
       nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
       dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
@@ -128,8 +138,15 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
       rve_sync<CL>();
       ns_from_rows<T>(gt, GNT, g, pl.cols, vrm, drm, nsv, dinv);
     }
-    // load cases: u = eps . x on the boundary, 0 inside
-    affine_soa<K>(gt, GNT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, false, u);
+    if constexpr (PER) {
+      // load cases: the fluctuation starts at 0; eps enters residual and averages
+      for (int i = t; i < SP_MAX_RHS * 6; i += NT)
+        seps[i] = (i < P.nrhs * 6) ? P.strains[(size_t)rid * P.nrhs * 6 + i] : 0.0;
+      for (size_t i = gt; i < (size_t)K * 3 * g.nn_pad; i += GNT) u[i] = 0.0;
+    } else {
+      // load cases: u = eps . x on the boundary, 0 inside
+      affine_soa<K>(gt, GNT, g, P.strains + (size_t)rid * P.nrhs * 6, P.nrhs, false, u);
+    }
     rve_sync<CL>();
 
     SolveArgs sa;
@@ -139,9 +156,10 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
     sa.warm = 0;
+    sa.eps = seps;
     sp_solve_info in;
     if constexpr (STENCIL) {
-      StencilOp<T, K> op{sKeT, etype};
+      StencilOp<T, K, PER> op{sKeT, etype};
       in = solve_rve<T, K, NT, CL>(g, op, dinv, etype, sKe, sD, sBbar, u, r, x, p, q, sa, red,
                                    &sh, savg);
     } else {
@@ -173,10 +191,12 @@ using BatchFn = void (*)(BatchParams);
   X(T, K, 512, 2, 8, SP_OP_ELL) \
   X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL) \
   X(T, K, 256, 2, 1, SP_OP_STENCIL) X(T, K, 256, 4, 1, SP_OP_STENCIL) \
-  X(T, K, 1024, 1, 1, SP_OP_STENCIL)
+  X(T, K, 1024, 1, 1, SP_OP_STENCIL) \
+  X(T, K, 512, 1, 1, SP_OP_STENCIL_PER) X(T, K, 512, 2, 1, SP_OP_STENCIL_PER)
 #define SP_BATCH_SHAPES_FP64(X, T, K) \
   X(T, K, 512, 1, 1, SP_OP_ELL) X(T, K, 512, 2, 1, SP_OP_ELL) \
-  X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL)
+  X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL) \
+  X(T, K, 512, 1, 1, SP_OP_STENCIL_PER) X(T, K, 512, 2, 1, SP_OP_STENCIL_PER)
 
 #define SP_BATCH_EXTERN(T, K, NT, MINB, CL, OP) \
   extern template __global__ void k_batch<T, K, NT, MINB, CL, OP>(BatchParams);

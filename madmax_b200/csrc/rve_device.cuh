@@ -28,6 +28,8 @@ struct MeshGeo {
   int nn, nn_pad;    // nodes, nodes rounded up to a multiple of 32
   double hx, hy, hz; // element edge lengths
   double vol;        // RVE volume
+  int periodic;      // periodic boundary conditions (unknowns on the periodic grid)
+  int pad;
 };
 
 __host__ __device__ inline bool is_bnode(const MeshGeo &g, int node) {
@@ -786,35 +788,62 @@ struct StencilAcc<double, K> {
   __device__ double get(int d, int q) const { return v[d][q]; }
 };
 
-// y = A x (K right-hand sides, component-major) with the stencil operator on
-// interior nodes; boundary and padding entries of y are not written.  A warp
-// takes 32 consecutive interior nodes (x fastest), a lane one node.  A warp
-// whose nodes all lie inside one material reads that material's assembled
-// blocks (one shared-memory broadcast per load); other warps sum each
-// neighbour block from the element blocks of their own materials.  Adds x.y
-// per load case into dot[K].
-template <typename T, int K>
+// y = A x (K right-hand sides, component-major) with the stencil operator.
+// Dirichlet (PER = false): interior nodes only; boundary and padding entries
+// of y are not written.  Periodic (PER): every node of the periodic grid,
+// neighbours and elements wrapped, y = 0 at the fixed node 0.  A warp takes
+// 32 consecutive nodes (x fastest), a lane one node.  A warp whose nodes all
+// lie inside one material reads that material's assembled blocks (one
+// shared-memory broadcast per load); other warps sum each neighbour block
+// from the element blocks of their own materials.  Adds x.y per load case
+// into dot[K].
+template <typename T, int K, bool PER = false>
 __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB,
                                     const uint8_t *__restrict__ etype, const T *x, T *y,
                                     double *dot) {
   using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
   const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
-  const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
+  const int mx = PER ? g.nex : g.nx - 2, my = PER ? g.ney : g.ny - 2, mz = PER ? g.nez : g.nz - 2;
   const int ni = mx * my * mz;
-  const int sy = g.nx, sz = g.nx * g.ny, esy = g.nex, esz = g.nex * g.ney;
+  // node strides of the vectors and of the element grid
+  const int sy = PER ? g.nex : g.nx, sz = PER ? g.nex * g.ney : g.nx * g.ny;
+  const int esy = g.nex, esz = g.nex * g.ney;
   const size_t blk = (size_t)3 * g.nn_pad;
   for (int s0 = warp * 32; s0 < ni; s0 += nwarps * 32) {
     const int id = s0 + lane;
     const bool valid = id < ni;
     const int idc = valid ? id : ni - 1;
-    const int i = 1 + idc % mx, j = 1 + (idc / mx) % my, k = 1 + idc / (mx * my);
+    const int ii = idc % mx, jj = (idc / mx) % my, kk = idc / (mx * my);
+    const int i = PER ? ii : ii + 1, j = PER ? jj : jj + 1, k = PER ? kk : kk + 1;
     const int a = i + j * sy + k * sz;
-    const int e0 = (i - 1) + (j - 1) * esy + (k - 1) * esz;
+    // periodic: offsets of the wrapped neighbours at -1 / +1 along each
+    // axis (index 0 / 1) and of the wrapped elements below the node
+    int xo[2], yo[2], zo[2], ex0 = i - 1, ey0 = j - 1, ez0 = k - 1;
+    if constexpr (PER) {
+      xo[0] = (i == 0) ? mx - 1 : -1;
+      xo[1] = (i == mx - 1) ? 1 - mx : 1;
+      yo[0] = ((j == 0) ? my - 1 : -1) * sy;
+      yo[1] = ((j == my - 1) ? 1 - my : 1) * sy;
+      zo[0] = ((k == 0) ? mz - 1 : -1) * sz;
+      zo[1] = ((k == mz - 1) ? 1 - mz : 1) * sz;
+      ex0 += (i == 0) ? g.nex : 0;
+      ey0 += (j == 0) ? g.ney : 0;
+      ez0 += (k == 0) ? g.nez : 0;
+    }
+    // neighbour (dx, dy, dz) of node a
+    auto nbr_of = [&](int dx, int dy, int dz) {
+      if constexpr (PER)
+        return a + (dx ? xo[dx > 0] : 0) + (dy ? yo[dy > 0] : 0) + (dz ? zo[dz > 0] : 0);
+      else
+        return a + dx + dy * sy + dz * sz;
+    };
     int tb[8];  // offset of the element's material blocks in KB
     unsigned mask = 0;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-      const unsigned te = __ldg(etype + e0 + (c & 1) + ((c >> 1) & 1) * esy + (c >> 2) * esz);
+      const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+      const int e = (ox ? i : ex0) + (oy ? j : ey0) * esy + (oz ? k : ez0) * esz;
+      const unsigned te = __ldg(etype + e);
       mask |= te << c;
       tb[c] = SP_KE_OFF + (int)te * SP_KB_TYPE;
     }
@@ -832,7 +861,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
           const int dx = mm % 3 - 1, dy = mm / 3 - 1;
           A bv[9] = {};
           add_block<T, A>(ka + ((dz + 1) * 9 + mm) * SP_KB_BLK, bv);
-          acc.fma_block(bv, x, blk, g.nn_pad, a + dx + dy * sy + dz * sz);
+          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz));
         }
       }
     } else {
@@ -856,7 +885,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
             const int lb = hex8_local(bx, by, 0) + 4 * bz;
             add_block<T, A>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK, bv);
           }
-          acc.fma_block(bv, x, blk, g.nn_pad, a + dx + dy * sy + dz * sz);
+          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz));
         }
       }
     }
@@ -866,7 +895,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           size_t o = q * blk + (size_t)d * g.nn_pad + a;
-          T yv = (T)acc.get(d, q);
+          T yv = (PER && a == 0) ? T(0) : (T)acc.get(d, q);
           dot[q] += (double)yv * (double)x[o];
           y[o] = yv;
         }
@@ -874,21 +903,166 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
   }
 }
 
+// ------------------------------------------------------ periodic BCs ---
+//
+// Periodic boundary conditions by master-slave elimination: u = eps.x + w
+// with the fluctuation w periodic, so the nodes at x = Lx (y = Ly, z = Lz)
+// are the images of those at 0 and the unknowns live on the periodic grid of
+// nex x ney x nez nodes, node i + nex (j + ney k).  All 8 corners are one
+// periodic node, node 0, whose w is fixed to 0: the corners carry eps.x, as
+// in the reference's 2D Lagrange-multiplier variant (micro/src/assembly.c:
+// 175-220, corners prescribed and opposite faces tied by u+ - u- = eps.dl),
+// and the rigid translations are removed.  The operator on w is P^T K P (the
+// stencil with wrapped neighbours and elements), the right-hand side
+// -P^T K (eps.x); u is never formed: residual and averages add eps.x per
+// element from the element's own (unwrapped) node coordinates.
+
+// component d of eps.x (engineering shears halved; micro/src/homogenize.c:
+// 335-342 in 3D)
+__device__ inline double affine_comp(const double *e, int d, double X, double Y, double Z) {
+  if (d == 0) return dadd(dadd(dmul(e[0], X), dmul(e[3] / 2, Y)), dmul(e[5] / 2, Z));
+  if (d == 1) return dadd(dadd(dmul(e[3] / 2, X), dmul(e[1], Y)), dmul(e[4] / 2, Z));
+  return dadd(dadd(dmul(e[5] / 2, X), dmul(e[4] / 2, Y)), dmul(e[2], Z));
+}
+
+// b = -P^T K (eps.x + P w) on the free periodic dofs, 0 at node 0 and on
+// padding; |b|^2 per load case into nrm2.  eps: [K][6] (shared).
+template <int K, typename R, bool SCALE = false>
+__device__ inline void residual_per(int t, int nt, const MeshGeo &g,
+                                    const uint8_t *__restrict__ etype,
+                                    const double *Ke /*[2][576], shared*/, const double *eps,
+                                    const double *__restrict__ w, R *rb, double *nrm2,
+                                    double *scale2 = nullptr) {
+  const size_t blk = (size_t)3 * g.nn_pad;
+  const int np = g.nelm;
+  for (int idx = t; idx < 3 * g.nn_pad; idx += nt) {
+    const int d = idx / g.nn_pad, node = idx % g.nn_pad;
+    double acc[K], mag[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) acc[q] = mag[q] = 0.0;
+    if (node > 0 && node < np) {
+      const int i = node % g.nex, j = (node / g.nex) % g.ney, k = node / (g.nex * g.ney);
+#pragma unroll 1
+      for (int c = 0; c < 8; c++) {
+        const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+        int ex = i - 1 + ox, ey = j - 1 + oy, ez = k - 1 + oz;
+        ex += (ex < 0) ? g.nex : 0;
+        ey += (ey < 0) ? g.ney : 0;
+        ez += (ez < 0) ? g.nez : 0;
+        const int e = ex + ey * g.nex + ez * g.nex * g.ney;
+        const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+        const double *ke = Ke + etype[e] * SP_KE + (la * 3 + d) * SP_NC;
+#pragma unroll 2
+        for (int b = 0; b < 8; b++) {
+          const int bx = ex + corner_x(b), by = ey + corner_y(b), bz = ez + corner_z(b);
+          const int nb = (bx == g.nex ? 0 : bx) + g.nex * ((by == g.ney ? 0 : by) +
+                                                           g.ney * (bz == g.nez ? 0 : bz));
+          const double X = bx * g.hx, Y = by * g.hy, Z = bz * g.hz;
+#pragma unroll
+          for (int db = 0; db < 3; db++) {
+            const double kv = ke[b * 3 + db];
+#pragma unroll
+            for (int q = 0; q < K; q++) {
+              const double uv = affine_comp(eps + q * 6, db, X, Y, Z) +
+                                w[q * blk + (size_t)db * g.nn_pad + nb];
+              acc[q] = fma(kv, uv, acc[q]);
+              if (SCALE) mag[q] += fabs(kv * uv);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      const double b = -acc[q];
+      rb[q * blk + idx] = (R)b;
+      nrm2[q] += b * b;
+      if (SCALE) scale2[q] += mag[q] * mag[q];
+    }
+  }
+}
+
+// Jacobi diagonal inverse of the periodic stencil operator; 0 at node 0 and
+// on padding.
+template <typename T>
+__device__ inline void stencil_dinv_per(int t, int nt, const MeshGeo &g,
+                                        const uint8_t *__restrict__ etype, const double *Ke,
+                                        T *dinv) {
+  for (int x = t; x < 3 * g.nn_pad; x += nt) {
+    const int d = x / g.nn_pad, node = x % g.nn_pad;
+    T v = T(0);
+    if (node > 0 && node < g.nelm) {
+      const int i = node % g.nex, j = (node / g.nex) % g.ney, k = node / (g.nex * g.ney);
+      double s = 0.0;
+      for (int c = 0; c < 8; c++) {
+        const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+        int ex = i - 1 + ox, ey = j - 1 + oy, ez = k - 1 + oz;
+        ex += (ex < 0) ? g.nex : 0;
+        ey += (ey < 0) ? g.ney : 0;
+        ez += (ez < 0) ? g.nez : 0;
+        const int e = ex + ey * g.nex + ez * g.nex * g.ney;
+        const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+        s += Ke[etype[e] * SP_KE + (3 * la + d) * SP_NC + 3 * la + d];
+      }
+      v = (T)(1.0 / s);
+    }
+    dinv[x] = v;
+  }
+}
+
+// volume averages of load case q under periodic conditions: u_e = eps.x_e +
+// w_e per element (see average_soa)
+__device__ inline void average_per(int t, int nt, const MeshGeo &g,
+                                   const uint8_t *__restrict__ etype, const double *D,
+                                   const double *Bbar, const double *eps_q,
+                                   const double *__restrict__ w, int q, double *acc) {
+  const size_t blk = (size_t)3 * g.nn_pad;
+  for (int e = t; e < g.nelm; e += nt) {
+    const int ex = e % g.nex, ey = (e / g.nex) % g.ney, ez = e / (g.nex * g.ney);
+    double eps[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int a = 0; a < 8; a++) {
+      const int bx = ex + corner_x(a), by = ey + corner_y(a), bz = ez + corner_z(a);
+      const int nb = (bx == g.nex ? 0 : bx) + g.nex * ((by == g.ney ? 0 : by) +
+                                                       g.ney * (bz == g.nez ? 0 : bz));
+      const double X = bx * g.hx, Y = by * g.hy, Z = bz * g.hz;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        const double uv = affine_comp(eps_q, d, X, Y, Z) + w[q * blk + (size_t)d * g.nn_pad + nb];
+#pragma unroll
+        for (int v = 0; v < 6; v++) eps[v] = fma(Bbar[v * 24 + a * 3 + d], uv, eps[v]);
+      }
+    }
+    const double *C = D + etype[e] * 36;
+#pragma unroll
+    for (int v = 0; v < 6; v++) {
+      double s = 0.0;
+#pragma unroll
+      for (int x = 0; x < 6; x++) s = fma(C[v * 6 + x], eps[x], s);
+      acc[v] += eps[v];
+      acc[6 + v] += s;
+    }
+  }
+}
+
 // b = -K u on interior dofs, 0 on the boundary and on padding (component-
 // major vectors; see residual_nodes for the arithmetic).  BCONLY: u's
 // interior values are read as 0, giving the right-hand side -K u_bc of the
-// load cases.
-template <int K, typename R, bool BCONLY = false>
+// load cases.  SCALE: also adds, per load case, the squared norm of the rows'
+// sums of term magnitudes into scale2[K] (the size below which b is
+// cancellation round-off).
+template <int K, typename R, bool BCONLY = false, bool SCALE = false>
 __device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
                                     const uint8_t *__restrict__ etype,
                                     const double *Ke /*[2][576], shared*/,
-                                    const double *__restrict__ u, R *rb, double *nrm2) {
+                                    const double *__restrict__ u, R *rb, double *nrm2,
+                                    double *scale2 = nullptr) {
   const size_t blk = (size_t)3 * g.nn_pad;
   for (int idx = t; idx < 3 * g.nn_pad; idx += nt) {
     int d = idx / g.nn_pad, node = idx % g.nn_pad;
-    double acc[K];
+    double acc[K], mag[K];
 #pragma unroll
-    for (int q = 0; q < K; q++) acc[q] = 0.0;
+    for (int q = 0; q < K; q++) acc[q] = mag[q] = 0.0;
     if (node < g.nn) {
       int i = node % g.nx, j = (node / g.nx) % g.ny, k = node / (g.nx * g.ny);
       bool bnd = (i == 0 || j == 0 || k == 0 || i == g.nx - 1 || j == g.ny - 1 || k == g.nz - 1);
@@ -910,8 +1084,11 @@ __device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
             for (int db = 0; db < 3; db++) {
               double kv = ke[b * 3 + db];
 #pragma unroll
-              for (int q = 0; q < K; q++)
-                acc[q] = fma(kv, u[q * blk + (size_t)db * g.nn_pad + nb], acc[q]);
+              for (int q = 0; q < K; q++) {
+                const double uv = u[q * blk + (size_t)db * g.nn_pad + nb];
+                acc[q] = fma(kv, uv, acc[q]);
+                if (SCALE) mag[q] += fabs(kv * uv);
+              }
             }
           }
         }
@@ -922,6 +1099,7 @@ __device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
       double b = -acc[q];
       rb[q * blk + idx] = (R)b;
       nrm2[q] += b * b;
+      if (SCALE) scale2[q] += mag[q] * mag[q];
     }
   }
 }

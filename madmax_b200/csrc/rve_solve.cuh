@@ -24,11 +24,16 @@ namespace sp {
 
 namespace cg = cooperative_groups;
 
+// A right-hand side whose norm is at most this fraction of the norm of its
+// summed term magnitudes is cancellation round-off of an exactly zero one.
+constexpr double SP_RHS_FLOOR = 1e-12;
+
 struct SolveArgs {
   int nrhs;
   double rtol, inner_rtol;
   int max_outer, max_inner;
   int warm;  // u's interior holds a start iterate other than 0
+  const double *eps;  // periodic conditions: [K][6] strains of the load cases (shared)
 };
 
 struct CgShared {
@@ -114,12 +119,12 @@ struct EllOp {
   }
 };
 
-template <typename T, int K>
+template <typename T, int K, bool PER = false>
 struct StencilOp {
   const T *kb;  // shared-memory element blocks (stencil_blocks)
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot) const {
-    spmm_stencil<T, K>(gt, gnt, g, kb, etype, p, q, dot);
+    spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot);
   }
 };
 
@@ -170,13 +175,17 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
     // The stopping rule is relative to the right-hand side, the residual of
     // the boundary values alone (not to the residual of the start iterate,
     // which a good warm start makes tiny).  A load case whose right-hand
-    // side vanishes has the solution 0 inside.
-    double m0[K];
+    // side vanishes (is round-off of cancelling terms) has the solution 0
+    // inside.
+    double m0[2 * K];
 #pragma unroll
-    for (int k = 0; k < K; k++) m0[k] = 0.0;
-    residual_soa<K, T, true>(gt, GNT, g, etype, sKe, u, r, m0);
-    rve_reduce<K, CL>(m0, red, sh);
-    if (warp == 0 && lane < K) sh->rn0[lane] = sqrt(red[32 * K + lane]);
+    for (int k = 0; k < 2 * K; k++) m0[k] = 0.0;
+    residual_soa<K, T, true, true>(gt, GNT, g, etype, sKe, u, r, m0, m0 + K);
+    rve_reduce<2 * K, CL>(m0, red, sh);
+    if (warp == 0 && lane < K) {
+      const double rn = sqrt(red[64 * K + lane]), sc = sqrt(red[64 * K + K + lane]);
+      sh->rn0[lane] = (rn <= SP_RHS_FLOOR * sc) ? 0.0 : rn;
+    }
     __syncthreads();
     for (int k = 0; k < P.nrhs; k++) {
       if (sh->rn0[k] > 0.0) continue;
@@ -186,18 +195,36 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
     rve_sync<CL>();
   }
   for (;;) {
-    // 3a. FP64 residual b = -K u -> r (type T) and its norms
+    // 3a. FP64 residual b = -K u -> r (type T) and its norms; on a cold
+    // start the first one is the right-hand side, whose norm the later
+    // ones are measured against (a right-hand side at the round-off level
+    // of its own cancelling terms is zero: that load case is solved)
     {
-      double m1[K];
+      const bool first = outer == 0 && !P.warm;
+      double m1[2 * K];
 #pragma unroll
-      for (int k = 0; k < K; k++) m1[k] = 0.0;
-      residual_soa<K, T>(gt, GNT, g, etype, sKe, u, r, m1);
-      rve_reduce<K, CL>(m1, red, sh);
+      for (int k = 0; k < 2 * K; k++) m1[k] = 0.0;
+      if (g.periodic) {
+        if (first)
+          residual_per<K, T, true>(gt, GNT, g, etype, sKe, P.eps, u, r, m1, m1 + K);
+        else
+          residual_per<K, T>(gt, GNT, g, etype, sKe, P.eps, u, r, m1);
+      } else {
+        if (first)
+          residual_soa<K, T, false, true>(gt, GNT, g, etype, sKe, u, r, m1, m1 + K);
+        else
+          residual_soa<K, T>(gt, GNT, g, etype, sKe, u, r, m1);
+      }
+      if (first)
+        rve_reduce<2 * K, CL>(m1, red, sh);
+      else
+        rve_reduce<K, CL>(m1, red, sh);
+      const int tot = first ? 64 * K : 32 * K;  // where rve_reduce left the totals
       if (warp == 0) {
         bool notdone = false;
         if (lane < K) {
-          double rn = sqrt(red[32 * K + lane]);
-          if (outer == 0 && !P.warm) sh->rn0[lane] = rn;
+          double rn = sqrt(red[tot + lane]);
+          if (first) sh->rn0[lane] = (rn <= SP_RHS_FLOOR * sqrt(red[tot + K + lane])) ? 0.0 : rn;
           sh->rn[lane] = rn;
           double rn0 = sh->rn0[lane];
           notdone = lane < P.nrhs && rn0 > 0.0 && rn > P.rtol * rn0;
@@ -331,7 +358,10 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
     double acc[12];
 #pragma unroll
     for (int v = 0; v < 12; v++) acc[v] = 0.0;
-    average_soa(gt, GNT, g, etype, sD, sBbar, u, qq, acc);
+    if (g.periodic)
+      average_per(gt, GNT, g, etype, sD, sBbar, P.eps + qq * 6, u, qq, acc);
+    else
+      average_soa(gt, GNT, g, etype, sD, sBbar, u, qq, acc);
     rve_reduce<12, CL>(acc, red, sh);
     if (t == 0)
       for (int v = 0; v < 12; v++) avg[qq * 12 + v] = red[32 * 12 + v] / g.vol;

@@ -276,6 +276,7 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
     sa.warm = warm;
+    sa.eps = nullptr;  // affine conditions: eps is carried by u's boundary values
     sp_solve_info in;
     if constexpr (STENCIL) {
       StencilOp<float, SERVE_K> op{sKB, G.etype};

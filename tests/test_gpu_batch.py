@@ -122,3 +122,68 @@ def test_stencil_and_assembled_agree_on_boxes():
 def test_unknown_batch_option_is_rejected():
     with pytest.raises(TypeError):
         mb.batch_opts(oprator=1)
+
+
+# ------------------------------------------------- periodic conditions ---
+
+from oracle import periodic as PER  # noqa: E402
+
+
+def test_periodic_tangents_match_oracle():
+    """Periodic (master-slave) conditions on the stencil path against the
+    CPU periodic oracle at 1e-8, in both precisions."""
+    descs = make_descs(31, [2, 3, 4, 5, 6, 8, 4])
+    for prec in (mb.SP_PREC_MIXED, mb.SP_PREC_FP64):
+        s, strain, info = mb.Batch(descs, bc=mb.SP_BC_PERIODIC, precision=prec).homogenize()
+        inf = mb.info_array(info)
+        assert (inf["status"] == 0).all() and (inf["relres"] <= 1e-8).all()
+        for i, d in enumerate(descs):
+            m = O.cube_mesh(d.n[0])
+            et = O.fiber_types(m, [1, 1], d.radius)
+            _, st, _ = PER.homogenize_periodic(m, et, (d.E[0], d.E[1]), (d.nu[0], d.nu[1]),
+                                               np.eye(6))
+            assert np.abs(s[i] - st).max() <= 1e-8 * np.abs(st).max(), (prec, i)
+            assert np.allclose(strain[i], np.eye(6), atol=1e-12)
+
+
+def test_periodic_homogeneous_box_gives_D():
+    """A homogeneous RVE (both materials equal) under periodic conditions is
+    a patch test: the fluctuation vanishes and <sigma> = D eps exactly, on
+    non-cubic boxes too."""
+    descs = make_descs(3, [3, 4, 5])
+    for d, n, ln in zip(descs, [(3, 4, 2), (4, 4, 4), (6, 2, 3)],
+                        [(1.0, 1.3, 0.7), (1.0, 1.0, 1.0), (2.0, 0.5, 1.0)]):
+        d.n[0], d.n[1], d.n[2] = n
+        d.len[0], d.len[1], d.len[2] = ln
+        d.E[1], d.nu[1] = d.E[0], d.nu[0]
+    s, _, info = mb.Batch(descs, bc=mb.SP_BC_PERIODIC).homogenize()
+    assert (mb.info_array(info)["status"] == 0).all()
+    for i, d in enumerate(descs):
+        D = np.zeros(36)
+        O.lib().orc_iso_D(3, d.E[0], d.nu[0], O.ptr(D))
+        assert np.abs(s[i] - D.reshape(6, 6)).max() <= 1e-9 * d.E[0], i
+
+
+def test_periodic_is_softer_than_affine():
+    """Hill bounds: C_affine - C_periodic is positive semi-definite."""
+    descs = make_descs(8, [6, 8])
+    sa, _, _ = mb.Batch(descs).homogenize()
+    sp, _, _ = mb.Batch(descs, bc=mb.SP_BC_PERIODIC).homogenize()
+    for i in range(len(descs)):
+        dC = sa[i].T - sp[i].T
+        ev = np.linalg.eigvalsh((dC + dC.T) / 2)
+        assert ev.min() >= -1e-7 * np.abs(sa[i]).max()
+        assert ev.max() > 1e-3 * np.abs(sa[i]).max()
+
+
+def test_periodic_rejects_assembled_operator_and_thin_meshes():
+    import ctypes as C
+    descs = make_descs(1, [4])
+    arr = (mb.sp_rve_desc * 1)(*descs)
+    h = mb._vp()
+    o = mb.batch_opts(bc=mb.SP_BC_PERIODIC, op=mb.SP_OP_ELL)
+    assert mb.lib().sp_batch_create(1, arr, C.byref(o), C.byref(h)) == mb.SP_ERR_ARG
+    descs[0].n[2] = 1
+    arr = (mb.sp_rve_desc * 1)(*descs)
+    o = mb.batch_opts(bc=mb.SP_BC_PERIODIC)
+    assert mb.lib().sp_batch_create(1, arr, C.byref(o), C.byref(h)) == mb.SP_ERR_ARG
