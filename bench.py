@@ -342,6 +342,7 @@ def run_ours(args):
                      cluster=args.cluster, inner_rtol=args.inner_rtol,
                      op=mb.SP_OP_STENCIL if args.op == "stencil" else mb.SP_OP_ELL)
     setup_s = time.time() - t0
+    shape = batch.shape()
 
     for _ in range(args.warmup):
         batch.launch(sptr)
@@ -420,7 +421,8 @@ def run_ours(args):
             "config": {"workload": f"batched tangent: {args.nrve} RVEs per GPU, n uniform in "
                                    f"{set(args.sizes)}, 6 unit-strain load cases, rtol 1e-8",
                        "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8,
-                       "precision": "mixed", "cta_threads": args.threads, "ctas_per_sm": args.ctas,
+                       "precision": "mixed", "cta_threads": shape[0], "ctas_per_sm": shape[1],
+                       "persistent_grid": shape[2],
                        "cluster": args.cluster, "inner_rtol": args.inner_rtol,
                        "operator": args.op,
                        "l2": l2_note(args, sizes, batch),
@@ -605,8 +607,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nrve", type=int, default=4096)
-    ap.add_argument("--threads", type=int, default=512)
-    ap.add_argument("--ctas", type=int, default=2)
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: the library's choice)")
+    ap.add_argument("--ctas", type=int, default=0, help="CTAs per SM (0: the library's choice)")
     ap.add_argument("--cluster", type=int, default=1)
     ap.add_argument("--inner-rtol", type=float, default=1e-4)
     ap.add_argument("--op", default="stencil", choices=["stencil", "ell"],

@@ -156,6 +156,22 @@ int sp_rve_homogenize(sp_rve *r, int nrhs, const double *strains, double rtol,
 /* 6x6 homogenized tangent C[i][j] = <sigma_i>(e_j) from six unit-strain load
  * cases solved together as one 6-rhs CG. */
 int sp_rve_tangent(sp_rve *r, double rtol, double *C, sp_solve_info *info);
+/* Fields of load case q of the last sp_rve_homogenize / sp_rve_tangent:
+ * per-element strain and stress [nelm][6] (Gauss-weighted means over the
+ * element, get_elem_properties of micro/src/homogenize.c:370-395), nodal
+ * displacement and last residual [ndof].  Any output may be NULL. */
+int sp_rve_fields(sp_rve *r, int q, double *strain_e, double *stress_e, double *u,
+                  double *residual);
+/* Writes base.pvtu and base_0.vtu (VTK XML, ascii) with the fields of load
+ * case q: the arrays of the reference's micro_pvtu (micro/src/output.c:
+ * 43-188). */
+int sp_rve_write_vtu(sp_rve *r, int q, const char *base);
+/* The VTK writer on host arrays of an n[0] x n[1] x n[2] hex8 box of edges
+ * len[3]: u, res [3*nn] (NULL: zeros), etype [nelm], strain_e, stress_e
+ * [nelm][6] (NULL: zeros). */
+int sp_vtu_write(const char *base, const int *n, const double *len, const double *u,
+                 const double *res, const unsigned char *etype, const double *strain_e,
+                 const double *stress_e);
 
 /* ------------------------------------------------------------------ batch */
 
@@ -178,9 +194,9 @@ typedef struct {
   double inner_rtol; /* FP32 CG reduction per refinement step (default 1e-4) */
   int max_outer;     /* refinement steps (default 8) */
   int max_inner;     /* CG iterations per step (default 4000) */
-  int threads;       /* threads per CTA (0: tuned) */
+  int threads;       /* threads per CTA (0: 1024 for the stencil, 512 otherwise) */
   int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
-  int ctas_per_sm;   /* resident CTAs per SM: 1 or 2 (512 threads), 2 or 4 (256) */
+  int ctas_per_sm;   /* resident CTAs per SM: 1 (1024 threads), 1 or 2 (512), 2 or 4 (256); 0: 1 or 2 */
   int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 (assembled) */
   int op;            /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int bc;            /* SP_BC_AFFINE (default) or SP_BC_PERIODIC (stencil only) */
@@ -211,6 +227,8 @@ int sp_batch_download(sp_batch *b, double *stress, double *strain, sp_solve_info
 /* upload + launch + download + synchronize: the end-to-end call. */
 int sp_batch_homogenize(sp_batch *b, const double *strains, const double *materials,
                         double *stress, double *strain, sp_solve_info *info, void *stream);
+/* The CTA shape and persistent grid the batch launches with. */
+int sp_batch_shape(const sp_batch *b, int *threads, int *ctas_per_sm, int *grid);
 /* Kernel launches made by the last sp_batch_launch (for accounting). */
 int sp_batch_last_launches(const sp_batch *b, int *launches);
 
@@ -264,6 +282,49 @@ int sp_server_stop(sp_server *s);
 int sp_server_replay(sp_server *s, int nreq, const int *geom, const double *strain,
                      const double *t_arrival, double *t_done, double *stress, double *tangent,
                      sp_solve_info *info, double timeout_s);
+
+/* --------------------------------------------------- macro-micro messages */
+
+/* The reference's coupling message (message_t, inc/comm.h:18-27), field for
+ * field: an MPI program's message_t buffer can be passed as an sp_message. */
+#define SP_MAX_VOIGT 6
+#define SP_ACTION_NULL 0               /* inc/comm.h:12-16 */
+#define SP_ACTION_MICRO_CALC_STRESS 1
+#define SP_ACTION_MICRO_CALC_C_TANGENT 2
+#define SP_ACTION_MICRO_CALC_RHO 3
+#define SP_ACTION_MICRO_END 4
+
+typedef struct {
+  int action;
+  int num_voigt;
+  double strain_mac[SP_MAX_VOIGT];
+  double stress_ave[SP_MAX_VOIGT];
+  double c_tangent_ave[SP_MAX_VOIGT * SP_MAX_VOIGT];
+  double rho;
+} sp_message;
+
+#define SP_MICRO_LINEAR 0 /* like the reference for linear materials: one FD tangent
+                             around zero, stress = C eps (micro/src/homogenize.c:3-21) */
+#define SP_MICRO_SOLVE 1  /* every stress / tangent request solved at its strain */
+
+/* One micro endpoint: answers messages for one geometry of a serving loop
+ * (micro/src/main.c:114-153).  rho is what ACTION_MICRO_CALC_RHO returns
+ * (the reference's constant is 1e7, micro/src/init.c:9). */
+typedef struct sp_micro_s sp_micro;
+int sp_micro_create(sp_server *srv, int geometry, int mode, double rho, sp_micro **out);
+int sp_micro_destroy(sp_micro *m);
+/* Fills the reply fields of msg for its action; SP_ERR_ARG for an unknown
+ * action or num_voigt != 6. */
+int sp_micro_handle(sp_micro *m, sp_message *msg);
+/* The request loop over a caller's transport: receive, answer, send the
+ * reply, until ACTION_MICRO_END (not answered).  The callbacks return 0 on
+ * success. */
+typedef int (*sp_message_recv)(sp_message *msg, void *ctx);
+typedef int (*sp_message_send)(const sp_message *msg, void *ctx);
+int sp_micro_serve(sp_micro *m, sp_message_recv recv, sp_message_send send, void *ctx,
+                   long long *handled);
+/* Serving-loop requests made so far. */
+int sp_micro_requests(const sp_micro *m, long long *requests);
 
 /* -------------------------------------------------------------------- FE2 */
 

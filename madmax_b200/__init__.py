@@ -75,6 +75,21 @@ class sp_server_opts(C.Structure):
                 ("idle_spin_limit", C.c_int), ("op", C.c_int), ("ctas_per_sm", C.c_int)]
 
 
+SP_ACTION_NULL, SP_ACTION_MICRO_CALC_STRESS, SP_ACTION_MICRO_CALC_C_TANGENT = 0, 1, 2
+SP_ACTION_MICRO_CALC_RHO, SP_ACTION_MICRO_END = 3, 4
+SP_MICRO_LINEAR, SP_MICRO_SOLVE = 0, 1
+
+
+class sp_message(C.Structure):
+    """message_t of the reference (inc/comm.h:18-27)."""
+    _fields_ = [("action", C.c_int), ("num_voigt", C.c_int), ("strain_mac", C.c_double * 6),
+                ("stress_ave", C.c_double * 6), ("c_tangent_ave", C.c_double * 36),
+                ("rho", C.c_double)]
+
+
+MESSAGE_RECV = C.CFUNCTYPE(C.c_int, C.POINTER(sp_message), C.c_void_p)
+MESSAGE_SEND = C.CFUNCTYPE(C.c_int, C.POINTER(sp_message), C.c_void_p)
+
 SP_FE2_LINEAR, SP_FE2_PER_GP, SP_FE2_MAX_ITS = 0, 1, 16
 
 
@@ -134,6 +149,15 @@ _PROTOS = {
     "sp_ell_pcg_noalloc": (C.c_int, [C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_double, C.c_int,
                                      _ip, _dp, _vp]),
     "sp_classify": (C.c_int, [C.POINTER(sp_rve_desc), _up]),
+    "sp_rve_fields": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp]),
+    "sp_micro_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.POINTER(_vp)]),
+    "sp_micro_destroy": (C.c_int, [_vp]),
+    "sp_micro_handle": (C.c_int, [_vp, C.POINTER(sp_message)]),
+    "sp_micro_serve": (C.c_int, [_vp, MESSAGE_RECV, MESSAGE_SEND, C.c_void_p,
+                                 C.POINTER(C.c_longlong)]),
+    "sp_micro_requests": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "sp_rve_write_vtu": (C.c_int, [_vp, C.c_int, C.c_char_p]),
+    "sp_vtu_write": (C.c_int, [C.c_char_p, _ip, _dp, _dp, _dp, _up, _dp, _dp]),
     "sp_fe2_desc_default": (None, [C.POINTER(sp_fe2_desc)]),
     "sp_fe2_create": (C.c_int, [C.POINTER(sp_fe2_desc), C.POINTER(_vp)]),
     "sp_fe2_run": (C.c_int, [_vp, C.POINTER(sp_fe2_info)]),
@@ -155,6 +179,7 @@ _PROTOS = {
                                   C.POINTER(_vp)]),
     "sp_batch_destroy": (C.c_int, [_vp]),
     "sp_batch_device_bytes": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "sp_batch_shape": (C.c_int, [_vp, _ip, _ip, _ip]),
     "sp_batch_upload": (C.c_int, [_vp, _dp, _dp, _vp]),
     "sp_batch_launch": (C.c_int, [_vp, _vp]),
     "sp_batch_download": (C.c_int, [_vp, _dp, _dp, C.POINTER(sp_solve_info), _vp]),
@@ -340,6 +365,17 @@ class Rve:
         check(lib().sp_rve_tangent(self.h, rtol, ptr(Cm), C.byref(info)), "sp_rve_tangent")
         return Cm.reshape(6, 6), info
 
+    def fields(self, q=0):
+        """(strain_e [nelm,6], stress_e [nelm,6], u [ndof], residual [ndof]) of
+        load case q of the last solve."""
+        se, st = np.zeros((self.nelm, 6)), np.zeros((self.nelm, 6))
+        u, r = np.zeros(self.ndof), np.zeros(self.ndof)
+        check(lib().sp_rve_fields(self.h, q, ptr(se), ptr(st), ptr(u), ptr(r)), "sp_rve_fields")
+        return se, st, u, r
+
+    def write_vtu(self, base: str, q=0):
+        check(lib().sp_rve_write_vtu(self.h, q, base.encode()), "sp_rve_write_vtu")
+
     def close(self):
         if self.h:
             lib().sp_rve_destroy(self.h)
@@ -376,6 +412,12 @@ class Batch:
         check(lib().sp_batch_create(self.n, self.descs, C.byref(self.opts), C.byref(self.h)),
               "sp_batch_create")
         self.nrhs = self.opts.nrhs
+
+    def shape(self):
+        """(threads per CTA, CTAs per SM, persistent grid)."""
+        t, c, g = C.c_int(), C.c_int(), C.c_int()
+        check(lib().sp_batch_shape(self.h, C.byref(t), C.byref(c), C.byref(g)), "sp_batch_shape")
+        return t.value, c.value, g.value
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

@@ -101,9 +101,9 @@ extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   o->inner_rtol = 1e-4;
   o->max_outer = 8;
   o->max_inner = 4000;
-  o->threads = 512;
+  o->threads = 0;      // chosen per operator at create time
   o->lanes_per_row = 0;
-  o->ctas_per_sm = 2;
+  o->ctas_per_sm = 0;
   o->cluster = 1;
   o->op = SP_OP_STENCIL;
   o->bc = SP_BC_AFFINE;
@@ -133,12 +133,17 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (o.precision != SP_PREC_MIXED && o.precision != SP_PREC_FP64)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown precision");
   // CTA shape: 512 threads x 1 or 2 CTAs per SM, 256 threads x 2 or 4, or
-  // (stencil operator) 1024 threads x 1
-  if (o.threads == 0) o.threads = 512;
+  // (stencil operator) 1024 threads x 1.  Unset: 1024 x 1 for the stencil
+  // under affine conditions (fastest on the mixed-size workloads measured),
+  // 512 x 2 otherwise.
+  const bool big = o.op == SP_OP_STENCIL && o.bc == SP_BC_AFFINE && o.cluster <= 1 &&
+                   o.precision == SP_PREC_MIXED;
+  if (o.threads == 0) o.threads = big ? 1024 : 512;
+  if (o.ctas_per_sm == 0) o.ctas_per_sm = (o.threads == 1024) ? 1 : 2;
   if (o.threads != 256 && o.threads != 512 && o.threads != 1024)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: threads must be 256, 512 or 1024");
-  if (o.threads == 1024) o.ctas_per_sm = 1;
-  if (o.ctas_per_sm == 0) o.ctas_per_sm = 2;
+  if (o.threads == 1024 && o.ctas_per_sm != 1)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: 1024-thread CTAs run 1 per SM");
   if (o.threads == 512 && o.ctas_per_sm != 1 && o.ctas_per_sm != 2)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: 512-thread CTAs run 1 or 2 per SM");
   if (o.threads == 256 && o.ctas_per_sm != 2 && o.ctas_per_sm != 4)
@@ -424,5 +429,13 @@ extern "C" int sp_batch_homogenize(sp_batch *b, const double *strains, const dou
 extern "C" int sp_batch_last_launches(const sp_batch *b, int *launches) {
   if (!b || !launches) return sp_set_error(SP_ERR_ARG, "null argument");
   *launches = b->last_launches;
+  return SP_OK;
+}
+
+extern "C" int sp_batch_shape(const sp_batch *b, int *threads, int *ctas_per_sm, int *grid) {
+  if (!b) return sp_set_error(SP_ERR_ARG, "null batch");
+  if (threads) *threads = b->o.threads;
+  if (ctas_per_sm) *ctas_per_sm = b->o.ctas_per_sm;
+  if (grid) *grid = b->grid;
   return SP_OK;
 }

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "pcg.cuh"
 #include "sp_cuda.h"
@@ -99,6 +100,33 @@ __global__ void __launch_bounds__(256)
     for (int v = 0; v < 12; v++) out[q * 12 + v] = tot[v] / g.vol;
 }
 
+// Per-element strain and stress of load case q (micro/src/homogenize.c:
+// 370-395, get_elem_properties): the Gauss-weighted means over the element,
+// Bbar u_e / vol_elm and D_t Bbar u_e / vol_elm; u is [ndof][K].
+template <int K>
+__global__ void k_elem_fields(MeshGeo g, const uint8_t *__restrict__ etype, const double *D,
+                              const double *Bbar, const double *__restrict__ u, int q,
+                              double *strain_e, double *stress_e) {
+  const double vol_elm = g.hx * g.hy * g.hz;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.nelm; e += gridDim.x * blockDim.x) {
+    int nod[8];
+    elem_nodes(g, e, nod);
+    double eps[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < 8; a++)
+      for (int d = 0; d < 3; d++) {
+        double uv = u[(size_t)(nod[a] * 3 + d) * K + q];
+        for (int v = 0; v < 6; v++) eps[v] = fma(Bbar[v * 24 + a * 3 + d], uv, eps[v]);
+      }
+    const double *C = D + etype[e] * 36;
+    for (int v = 0; v < 6; v++) {
+      double sv = 0.0;
+      for (int w = 0; w < 6; w++) sv = fma(C[v * 6 + w], eps[w], sv);
+      strain_e[(size_t)e * 6 + v] = eps[v] / vol_elm;
+      stress_e[(size_t)e * 6 + v] = sv / vol_elm;
+    }
+  }
+}
+
 static int blocks_for(Device *d, long long items, int per_block) {
   long long b = (items + per_block - 1) / per_block;
   long long cap = (long long)d->nsm * 4;
@@ -128,6 +156,7 @@ struct sp_rve_s {
   PcgGraph<double, 6, 32> *pcg6 = nullptr;
   PcgGraph<double, 8, 32> *pcg8 = nullptr;
   size_t bytes = 0;
+  int last_k = 0, last_nrhs = 0;  // padded and actual load cases of the last solve
 };
 
 static int rve_assemble(sp_rve *r, Device *d, cudaStream_t s) {
@@ -343,6 +372,8 @@ static int rve_solve_k(sp_rve *r, Device *d, PcgGraph<double, K, 32> *&pcg, int 
     if (rel > worst) worst = rel;
   }
   r->last_launches = launches;
+  r->last_k = K;
+  r->last_nrhs = nrhs;
   int status = (worst <= rtol) ? SP_OK : SP_ERR_NOCONV;
   if (info) {
     info->status = status;
@@ -376,4 +407,48 @@ extern "C" int sp_rve_tangent(sp_rve *r, double rtol, double *C, sp_solve_info *
   for (int i = 0; i < 6; i++)
     for (int j = 0; j < 6; j++) C[i * 6 + j] = st[j * 6 + i];
   return rc;
+}
+
+extern "C" int sp_rve_fields(sp_rve *r, int q, double *strain_e, double *stress_e, double *u,
+                             double *residual) {
+  if (!r) return sp_set_error(SP_ERR_ARG, "sp_rve_fields: null rve");
+  if (r->last_nrhs < 1) return sp_set_error(SP_ERR_STATE, "sp_rve_fields: no solve yet");
+  if (q < 0 || q >= r->last_nrhs)
+    return sp_set_error(SP_ERR_RANGE, "sp_rve_fields: load case %d of %d", q, r->last_nrhs);
+  Device *d;
+  SP_TRY(device(&d));
+  cudaStream_t s = d->stream;
+  const MeshGeo &g = r->g;
+  const size_t ne = (size_t)g.nelm * 6;
+  double *dev = nullptr;
+  SP_TRY(dmalloc((void **)&dev, 2 * ne * sizeof(double), nullptr));
+  int nb = blocks_for(d, g.nelm, 256);
+  switch (r->last_k) {
+    case 1: k_elem_fields<1><<<nb, 256, 0, s>>>(g, r->d_etype, r->d_D, r->d_Bbar, r->d_u, q, dev, dev + ne); break;
+    case 6: k_elem_fields<6><<<nb, 256, 0, s>>>(g, r->d_etype, r->d_D, r->d_Bbar, r->d_u, q, dev, dev + ne); break;
+    default: k_elem_fields<8><<<nb, 256, 0, s>>>(g, r->d_etype, r->d_D, r->d_Bbar, r->d_u, q, dev, dev + ne); break;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (!e && strain_e) e = cudaMemcpyAsync(strain_e, dev, ne * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (!e && stress_e) e = cudaMemcpyAsync(stress_e, dev + ne, ne * sizeof(double), cudaMemcpyDeviceToHost, s);
+  // u and the last residual are [ndof][K]: one strided column each
+  if (!e && u)
+    e = cudaMemcpy2DAsync(u, sizeof(double), r->d_u + q, r->last_k * sizeof(double), sizeof(double),
+                          g.ndof, cudaMemcpyDeviceToHost, s);
+  if (!e && residual)
+    e = cudaMemcpy2DAsync(residual, sizeof(double), r->d_b + q, r->last_k * sizeof(double),
+                          sizeof(double), g.ndof, cudaMemcpyDeviceToHost, s);
+  if (!e) e = cudaStreamSynchronize(s);
+  cudaFree(dev);
+  if (e) return sp_set_error(SP_ERR_CUDA, "sp_rve_fields: %s", cudaGetErrorString(e));
+  return SP_OK;
+}
+
+extern "C" int sp_rve_write_vtu(sp_rve *r, int q, const char *base) {
+  if (!r || !base) return sp_set_error(SP_ERR_ARG, "sp_rve_write_vtu: null argument");
+  const MeshGeo &g = r->g;
+  std::vector<double> se((size_t)g.nelm * 6), st((size_t)g.nelm * 6), u(g.ndof), res(g.ndof);
+  SP_TRY(sp_rve_fields(r, q, se.data(), st.data(), u.data(), res.data()));
+  return sp_vtu_write(base, r->desc.n, r->desc.len, u.data(), res.data(), r->etype_h, se.data(),
+                      st.data());
 }

@@ -23,6 +23,13 @@ extern "C" {
 /* thread-local last error; returns code */
 int sp_set_error(int code, const char *fmt, ...);
 
+/* return a non-zero code from C host code */
+#define SP_TRY_C(x)        \
+  do {                     \
+    int sp_rc_ = (x);      \
+    if (sp_rc_) return sp_rc_; \
+  } while (0)
+
 /* Structured 3D mesh plan, shared by every RVE of the same mesh. */
 typedef struct {
   int n[3];            /* elements per axis */

@@ -82,7 +82,7 @@ def test_same_result_alone_and_in_mix():
     (512, 1, 1, mb.SP_OP_ELL), (512, 2, 1, mb.SP_OP_ELL), (256, 2, 1, mb.SP_OP_ELL),
     (256, 4, 1, mb.SP_OP_ELL), (512, 2, 2, mb.SP_OP_ELL), (512, 1, 4, mb.SP_OP_ELL),
     (512, 2, 8, mb.SP_OP_ELL), (512, 1, 1, mb.SP_OP_STENCIL), (512, 2, 1, mb.SP_OP_STENCIL),
-    (256, 2, 1, mb.SP_OP_STENCIL), (256, 4, 1, mb.SP_OP_STENCIL)])
+    (256, 2, 1, mb.SP_OP_STENCIL), (256, 4, 1, mb.SP_OP_STENCIL), (1024, 1, 1, mb.SP_OP_STENCIL)])
 def test_cta_shapes_agree(threads, ctas, cluster, op):
     """Every CTA shape, and RVEs split over thread-block clusters of 2, 4
     and 8 CTAs, give the oracle's result."""
@@ -187,3 +187,11 @@ def test_periodic_rejects_assembled_operator_and_thin_meshes():
     arr = (mb.sp_rve_desc * 1)(*descs)
     o = mb.batch_opts(bc=mb.SP_BC_PERIODIC)
     assert mb.lib().sp_batch_create(1, arr, C.byref(o), C.byref(h)) == mb.SP_ERR_ARG
+
+
+def test_default_shape_per_operator():
+    descs = make_descs(2, [4, 5])
+    assert mb.Batch(descs).shape()[:2] == (1024, 1)
+    assert mb.Batch(descs, op=mb.SP_OP_ELL).shape()[:2] == (512, 2)
+    assert mb.Batch(descs, bc=mb.SP_BC_PERIODIC).shape()[:2] == (512, 2)
+    assert mb.Batch(descs, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 2)

@@ -93,3 +93,38 @@ def test_non_cubic_mesh_and_offset_fiber():
     gsa, gst, gu, info = r.homogenize(eps, want_u=True)
     assert info.status == 0
     assert np.abs(gst - st).max() <= 1e-8 * np.abs(st).max()
+
+
+def test_element_fields_and_vtu_match_oracle(tmp_path):
+    """Per-element strain/stress (get_elem_properties, micro/src/homogenize.c:
+    370-395) of the second load case against the oracle's solution, their
+    volume average against the homogenized stress, and the VTU piece."""
+    import xml.etree.ElementTree as ET
+    n, rad, E, nu = 5, 0.3, (1e9, 2e10), (0.3, 0.2)
+    d = mb.rve_desc(n, rad, E, nu)
+    r = mb.Rve(d)
+    strains = np.array([[1e-3, 0, 0, 0, 0, 0], [2e-4, -1e-4, 3e-4, 1e-4, 0.0, -2e-4]])
+    _, st, _, info = r.homogenize(strains, rtol=1e-10)
+    se, ss, u, res = r.fields(1)
+    m = O.cube_mesh(n)
+    et = O.fiber_types(m, [1, 1], rad)
+    _, sto, uo, _ = O.homogenize(m, et, E, nu, strains, want_u=True, rtol=1e-12, lin_rtol=1e-13)
+    D, _, bmat, wp = O.operators(m, E, nu)
+    B = bmat.reshape(6, 24, 8)
+    dofs = O.elem_dofs(m)
+    eps_o = np.einsum("vig,ei,g->ev", B, uo[1][dofs], wp) / m.vol_elm
+    sig_o = np.einsum("evw,ew->ev", D[et], eps_o)
+    assert np.abs(u - uo[1]).max() <= 1e-8 * np.abs(uo[1]).max()
+    assert np.abs(se - eps_o).max() <= 1e-8 * np.abs(eps_o).max()
+    assert np.abs(ss - sig_o).max() <= 1e-8 * np.abs(sig_o).max()
+    assert np.abs(ss.mean(0) - st[1]).max() <= 1e-10 * np.abs(st[1]).max()
+    base = str(tmp_path / "micro")
+    r.write_vtu(base, 1)
+    v = ET.parse(base + "_0.vtu").getroot()
+    arr = {da.get("Name"): np.array(da.text.split(), dtype=float) for da in v.iter("DataArray")}
+    assert np.allclose(arr["displ"], u, rtol=1e-8, atol=1e-30)
+    assert np.allclose(arr["stress"].reshape(-1, 6), ss, rtol=1e-8, atol=1e-30)
+    assert (arr["elem_type"] == et).all()
+    with pytest.raises(mb.SputnikError):
+        r.fields(2)
+    r.close()

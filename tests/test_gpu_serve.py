@@ -131,3 +131,76 @@ def test_repeated_and_zero_strain_requests_converge():
     assert np.abs(st0).max() <= 1e-9 * np.abs(st1).max()
     assert np.abs(tg0 - tg1).max() <= 1e-7 * np.abs(tg1).max()
     assert np.abs(tg0b - tg1).max() <= 1e-7 * np.abs(tg1).max()
+
+
+# --------------------------------------- message_t coupling (micro side) ---
+
+def fake_transport(inbox):
+    """In-memory stand-in for the MPI transport: recv pops the next queued
+    message, send records the reply."""
+    sent = []
+
+    def recv(msg, ctx):
+        if not inbox:
+            return 1
+        C.memmove(msg, C.byref(inbox.pop(0)), C.sizeof(mb.sp_message))
+        return 0
+
+    def send(msg, ctx):
+        m = mb.sp_message()
+        C.memmove(C.byref(m), msg, C.sizeof(mb.sp_message))
+        sent.append(m)
+        return 0
+
+    return mb.MESSAGE_RECV(recv), mb.MESSAGE_SEND(send), sent
+
+
+def message(action, strain=None):
+    m = mb.sp_message()
+    m.action, m.num_voigt = action, 6
+    if strain is not None:
+        m.strain_mac[:] = list(strain)
+    return m
+
+
+@pytest.mark.parametrize("mode", [mb.SP_MICRO_SOLVE, mb.SP_MICRO_LINEAR])
+def test_micro_message_loop_matches_oracle(mode):
+    """The request loop of micro/src/main.c:114-153 over message_t: stress,
+    tangent and density requests answered from the serving loop, END ends
+    the loop unanswered; results against the oracle's FD tangent."""
+    G = geoms()
+    s = mb.Server(G)
+    s.start()
+    h = mb._vp()
+    mb.check(mb.lib().sp_micro_create(s.h, 4, mode, 1e7, C.byref(h)), "sp_micro_create")
+    e = np.array([4e-4, -2e-4, 1e-4, 3e-4, -1e-4, 2e-4])
+    inbox = [message(mb.SP_ACTION_MICRO_CALC_STRESS, e), message(mb.SP_ACTION_MICRO_CALC_C_TANGENT, e),
+             message(mb.SP_ACTION_MICRO_CALC_RHO), message(mb.SP_ACTION_MICRO_END)]
+    recv, send, sent = fake_transport(inbox)
+    n = C.c_longlong()
+    mb.check(mb.lib().sp_micro_serve(h, recv, send, None, C.byref(n)), "sp_micro_serve")
+    assert n.value == 4 and len(sent) == 3 and not inbox
+    assert [m.action for m in sent] == [1, 2, 3]
+    stress = np.array(sent[0].stress_ave[:])
+    tangent = np.array(sent[1].c_tangent_ave[:]).reshape(6, 6)
+    assert sent[2].rho == 1e7
+    s0, Cm = oracle_fd(G[4], e)
+    _, C0 = oracle_fd(G[4], np.zeros(6))
+    if mode == mb.SP_MICRO_SOLVE:
+        assert np.abs(stress - s0).max() <= 1e-8 * np.abs(s0).max()
+        assert np.abs(tangent - Cm).max() <= 1e-7 * np.abs(Cm).max()
+    else:
+        # the reference's linear path: C from the FD tangent around zero, sigma = C eps
+        assert np.abs(tangent - C0).max() <= 1e-7 * np.abs(C0).max()
+        assert np.abs(stress - C0 @ e).max() <= 1e-7 * np.abs(C0 @ e).max()
+    req = C.c_longlong()
+    mb.lib().sp_micro_requests(h, C.byref(req))
+    assert req.value == (2 if mode == mb.SP_MICRO_SOLVE else 1)
+    bad = message(9)
+    assert mb.lib().sp_micro_handle(h, C.byref(bad)) == mb.SP_ERR_ARG
+    bad = message(mb.SP_ACTION_MICRO_CALC_STRESS, e)
+    bad.num_voigt = 3
+    assert mb.lib().sp_micro_handle(h, C.byref(bad)) == mb.SP_ERR_ARG
+    mb.lib().sp_micro_destroy(h)
+    s.stop()
+    s.close()
