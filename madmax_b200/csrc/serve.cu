@@ -17,7 +17,9 @@
 //     kernel (rve_solve.cuh) -- on the element-type stencil (default) or on
 //     the geometry's resident FP32 ELL matrix -- warm-started from that
 //     geometry's previous solution, writes the result to mapped memory and
-//     raises the request's done flag.
+//     raises the request's done flag.  The warm start is a first-order
+//     prediction from the previous request's 7 solutions (u(eps) and
+//     u(eps + delta e_i) give the derivative of u in every strain direction).
 // A request is picked up as soon as any slot is free, while other requests
 // are still solving: their work overlaps on the device.  Every wait is
 // bounded (idle_spin_limit polls); on expiry the CTA returns and the host
@@ -51,7 +53,8 @@ struct ServeGeom {
   double *Ke;   // [2][576]
   double *D;    // [72]
   double *Bbar; // [144]
-  double *warm; // [8][3][nn_pad]
+  double *warm;     // [SERVE_K][3][nn_pad] solutions of the previous request
+  double *warm_eps; // [SERVE_K][6] its load-case strains
   const int *color_elems;
   const uint8_t *slot;
   int color_off[9];
@@ -156,6 +159,7 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
   __shared__ double red[33 * 16];
   __shared__ double savg[SP_MAX_RHS * 12];
   __shared__ double seps[SERVE_K * 6];
+  __shared__ double spred[SERVE_K * 6];  // warm-start predictor coefficients
   __shared__ CgShared sh;
   __shared__ long long s_job;
   __shared__ int s_geom;
@@ -260,11 +264,36 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     for (int i = t; i < 2 * SP_KE; i += SERVE_NT) sKe[i] = G.Ke[i];
     for (int i = t; i < 72; i += SERVE_NT) sD[i] = G.D[i];
     for (int i = t; i < 144; i += SERVE_NT) sB[i] = G.Bbar[i];
-    // warm start: previous solution of this geometry inside, eps . x on the boundary
+    // warm start from the geometry's previous request, whose solutions are
+    // u(e0) and u(e0 + d e_i), i = 0..5: the first-order predictor
+    //   u(e) ~ u(e0) + sum_i (e - e0)_i (u(e0 + d e_i) - u(e0)) / d
+    // (exact for linear materials up to the previous solves' tolerance) for
+    // every load case inside; eps . x on the boundary (below)
     const size_t nu = (size_t)SERVE_K * 3 * g.nn_pad;
     const bool warm = *(volatile int *)&G.has_warm;
-    if (warm)
-      for (size_t i = t; i < nu; i += SERVE_NT) u[i] = __ldcg(G.warm + i);
+    if (warm) {
+      if (t < SERVE_K * 6) {
+        const int k = t / 6, j = t % 6;
+        const double e0 = __ldcg(G.warm_eps + j);
+        const double d = __ldcg(G.warm_eps + (j + 1) * 6 + j) - e0;
+        spred[t] = (d != 0.0) ? (seps[k * 6 + j] - e0) / d : 0.0;
+      }
+      __syncthreads();
+      const size_t blk = (size_t)3 * g.nn_pad;
+      for (size_t i = t; i < blk; i += SERVE_NT) {
+        const double w0 = __ldcg(G.warm + i);
+        double dw[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) dw[j] = __ldcg(G.warm + (j + 1) * blk + i) - w0;
+#pragma unroll
+        for (int k = 0; k < SERVE_K; k++) {
+          double v = w0;
+#pragma unroll
+          for (int j = 0; j < 6; j++) v = fma(spred[k * 6 + j], dw[j], v);
+          u[k * blk + i] = v;
+        }
+      }
+    }
     __syncthreads();
     if constexpr (STENCIL) stencil_blocks<float>(t, SERVE_NT, sKe, sKB);
     affine_soa<SERVE_K>(t, SERVE_NT, g, seps, SERVE_NRHS, warm, u);
@@ -287,8 +316,9 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
       in = solve_rve<float, SERVE_K, SERVE_NT, 1>(g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p,
                                                   q, sa, red, &sh, savg);
     }
-    // keep this solution as the geometry's next warm start
+    // keep this request's solutions and strains as the geometry's next warm start
     for (size_t i = t; i < nu; i += SERVE_NT) __stcg(G.warm + i, u[i]);
+    if (t < SERVE_K * 6) __stcg(G.warm_eps + t, seps[t]);
     __threadfence();
     __syncthreads();
     if (t == 0) {
@@ -320,7 +350,7 @@ static size_t geom_bytes(const sp_rve_desc &d, int op) {
   size_t nn = (size_t)(d.n[0] + 1) * (d.n[1] + 1) * (d.n[2] + 1), np = (nn + 31) / 32 * 32;
   size_t nelm = (size_t)d.n[0] * d.n[1] * d.n[2];
   return (op == SP_OP_ELL ? np * 243 * 4 : 0) + 3 * np * 4 + nelm +
-         (2 * SP_KE + 72 + 144) * 8 + SERVE_K * 3 * np * 8 + 1024;
+         (2 * SP_KE + 72 + 144) * 8 + SERVE_K * (3 * np + 6) * 8 + 1024;
 }
 
 }  // namespace sp
@@ -487,7 +517,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
     size_t np = G.g.nn_pad, ne = G.g.nelm;
     void *b[7] = {};
     size_t sz[7] = {o.op == SP_OP_ELL ? np * 243 * 4 : 0, 3 * np * 4, ne + 16, 2 * SP_KE * 8,
-                    72 * 8, 144 * 8, SERVE_K * 3 * np * 8};
+                    72 * 8, 144 * 8, SERVE_K * (3 * np + 6) * 8};
     for (int k = 0; k < 7 && !rc; k++) {
       if (!sz[k]) continue;
       rc = dmalloc(&b[k], sz[k], &s->bytes);
@@ -501,6 +531,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
     G.D = (double *)b[4];
     G.Bbar = (double *)b[5];
     G.warm = (double *)b[6];
+    G.warm_eps = G.warm + (size_t)SERVE_K * 3 * np;
     std::vector<uint8_t> et(ne);
     rc = sp_classify_elements(&dd, et.data(), nullptr);
     if (!rc && cudaMemcpy((void *)G.etype, et.data(), ne, cudaMemcpyHostToDevice))
