@@ -202,7 +202,7 @@ def measure_spmv(mb, stream, sptr, n=40, reps=20):
                 "lanes_per_row": best, "ms": per[best],
                 "ms_by_lanes": {str(k): round(v, 4) for k, v in per.items()},
                 "algorithmic_bytes": abytes,
-                "traffic": profiled_traffic("k_spmv_rve_n40_fp64.md", f"structured ELL n={n} lanes 8"),
+                "traffic": profiled_traffic("k_spmv_rve_n40_fp64.md", f"structured ELL n={n}"),
                 "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_kind": peak_kind, "max_rel_err_vs_numpy": err}
     finally:
