@@ -308,6 +308,35 @@ def mix_rate(per_size_times):
     return 1.0 / mean_t
 
 
+def rank_seed(rank: int) -> int:
+    """Seed of a rank's workload: every rank solves its own RVEs (weak scaling,
+    no data exchange)."""
+    return 1234 + rank
+
+
+def max_over_ranks(dist, value: float, device) -> float:
+    """The largest per-rank value (device time of the same steps); every rank
+    takes part, in the same order, in warm-up, timing and error paths alike."""
+    import torch
+    if dist is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, nrve: int, steps: int, total_ms: float) -> float:
+    """RVE solves per second of the whole job: every rank's RVEs over the
+    slowest rank's time."""
+    return world * nrve * steps / (total_ms / 1000.0)
+
+
+def workload_config(args, sizes):
+    return {"workload": f"batched tangent: {args.nrve} RVEs per GPU, n uniform in "
+                        f"{set(args.sizes)}, 6 unit-strain load cases, rtol 1e-8",
+            "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -330,8 +359,9 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": "batched tangent: 4096 RVEs, n in {8,12,16,20}, 6 load cases",
-                   "sample_rves_per_step": per_step, "solver": "FP64 Jacobi-PCG (oracle port)"},
+        "config": {**workload_config(args, args.sizes),
+                   "sample_rves_per_step": per_step, "solver": "FP64 Jacobi-PCG (oracle port)",
+                   "parallelism": f"rank 0 of {args.gpus}: all host cores"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{per_step} seeded RVEs of the workload mix per step, "
                                    f"spawned process pool, one process per core"},
@@ -365,7 +395,7 @@ def run_ours(args):
     sptr = C.c_void_p(stream.cuda_stream)
     assert sptr.value, "expected a non-default stream"
 
-    descs = workload_descs(mb, args.nrve, 1234 + rank, tuple(args.sizes))
+    descs = workload_descs(mb, args.nrve, rank_seed(rank), tuple(args.sizes))
     sizes = [d.n[0] for d in descs]
     t0 = time.time()
     batch = mb.Batch(descs, nrhs=6, threads=args.threads, ctas_per_sm=args.ctas,
@@ -395,12 +425,8 @@ def run_ours(args):
         dist.barrier()
     clocks = sampler.stop()
     per_launch_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
-    total_ms = sum(per_launch_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.nrve * args.steps / (total_ms / 1000.0)
+    total_ms = max_over_ranks(dist, sum(per_launch_ms), "cuda")
+    value = whole_job_rate(world, args.nrve, args.steps, total_ms)
 
     stress = np.zeros((args.nrve, 6, 6))
     info = (mb.sp_solve_info * args.nrve)()
@@ -428,12 +454,9 @@ def run_ours(args):
         batch.download(h_stress, None, h_info, sptr)
         ee[2 * k + 1].record(stream)
         stream.synchronize()
-    e2e_ms = sum(ee[2 * k].elapsed_time(ee[2 * k + 1]) for k in range(args.e2e_steps))
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * args.nrve * args.e2e_steps / (e2e_ms / 1000.0)
+    e2e_ms = max_over_ranks(dist, sum(ee[2 * k].elapsed_time(ee[2 * k + 1])
+                                       for k in range(args.e2e_steps)), "cuda")
+    e2e_value = whole_job_rate(world, args.nrve, args.e2e_steps, e2e_ms)
     h2d = h_strain.nbytes + h_mats.nbytes
     d2h = h_stress.nbytes + C.sizeof(h_info)
 
@@ -448,9 +471,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": avg_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 CG + f64 refinement", "data": "synthetic",
-            "config": {"workload": f"batched tangent: {args.nrve} RVEs per GPU, n uniform in "
-                                   f"{set(args.sizes)}, 6 unit-strain load cases, rtol 1e-8",
-                       "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8,
+            "config": {**workload_config(args, sizes),
                        "precision": "mixed", "cta_threads": shape[0], "ctas_per_sm": shape[1],
                        "persistent_grid": shape[2],
                        "cluster": args.cluster, "inner_rtol": args.inner_rtol,
