@@ -296,17 +296,21 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         double m2[2 * K];
 #pragma unroll
         for (int k = 0; k < 2 * K; k++) m2[k] = 0.0;
+        // chunk-major: the diagonal is read once per chunk and the K load
+        // cases' loads of one chunk are independent of each other
+        T al[K];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-          const T al = (T)sh->alpha[k];
-          for (int c = gt; c < nch; c += GNT) {
-            size_t o = (size_t)k * blk + (size_t)c * E;
+        for (int k = 0; k < K; k++) al[k] = (T)sh->alpha[k];
+        for (int c = gt; c < nch; c += GNT) {
+          const W dv = W::load(dinv + (size_t)c * E);
+#pragma unroll
+          for (int k = 0; k < K; k++) {
+            const size_t o = (size_t)k * blk + (size_t)c * E;
             W xv = W::load(x + o), pv = W::load(p + o), rv = W::load(r + o), qv = W::load(q + o);
-            W dv = W::load(dinv + (size_t)c * E);
 #pragma unroll
             for (int e = 0; e < E; e++) {
-              xv.v[e] += al * pv.v[e];
-              rv.v[e] -= al * qv.v[e];
+              xv.v[e] += al[k] * pv.v[e];
+              rv.v[e] -= al[k] * qv.v[e];
               m2[k] += (double)rv.v[e] * (double)(dv.v[e] * rv.v[e]);
               m2[K + k] += (double)rv.v[e] * (double)rv.v[e];
             }
@@ -332,16 +336,21 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
       }
       it++;
       if (sh->nact == 0) break;
-      // p = D^-1 r + beta p
+      // p = D^-1 r + beta p (chunk-major as above)
+      {
+        T be[K];
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        const T be = (T)sh->beta[k];
+        for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
         for (int c = gt; c < nch; c += GNT) {
-          size_t o = (size_t)k * blk + (size_t)c * E;
-          W rv = W::load(r + o), pv = W::load(p + o), dv = W::load(dinv + (size_t)c * E);
+          const W dv = W::load(dinv + (size_t)c * E);
 #pragma unroll
-          for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be * pv.v[e];
-          pv.store(p + o);
+          for (int k = 0; k < K; k++) {
+            const size_t o = (size_t)k * blk + (size_t)c * E;
+            W rv = W::load(r + o), pv = W::load(p + o);
+#pragma unroll
+            for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be[k] * pv.v[e];
+            pv.store(p + o);
+          }
         }
       }
       rve_sync<CL>();  // the next SpMM gathers p rows of every CTA
