@@ -195,3 +195,48 @@ def test_default_shape_per_operator():
     assert mb.Batch(descs, op=mb.SP_OP_ELL).shape()[:2] == (512, 2)
     assert mb.Batch(descs, bc=mb.SP_BC_PERIODIC).shape()[:2] == (512, 2)
     assert mb.Batch(descs, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 2)
+
+
+# --------------------------------------------------- edge and full sizes ---
+
+def test_single_element_and_thin_meshes():
+    """n = 1 (every node on the boundary: nothing to solve) and meshes one
+    element thick agree with the oracle; an empty batch is refused."""
+    import ctypes as C
+    descs = make_descs(12, [1, 2, 1])
+    descs[1].n[0], descs[1].n[1], descs[1].n[2] = 1, 3, 2
+    s, strain, info = mb.Batch(descs).homogenize()
+    inf = mb.info_array(info)
+    assert (inf["status"] == 0).all() and (inf["inner"][[0, 2]] == 0).all()
+    for i in (0, 2):
+        d = descs[i]
+        m = O.cube_mesh(1)
+        et = O.fiber_types(m, [1, 1], d.radius)
+        _, st, _, _ = O.homogenize(m, et, (d.E[0], d.E[1]), (d.nu[0], d.nu[1]), np.eye(6),
+                                   rtol=1e-12, lin_rtol=1e-13)
+        assert np.abs(s[i] - st).max() <= 1e-8 * np.abs(st).max()
+    e, _, _ = mb.Batch([descs[1]], op=mb.SP_OP_ELL).homogenize()
+    assert np.abs(s[1] - e[0]).max() <= 2e-8 * np.abs(e[0]).max()
+    h = mb._vp()
+    arr = (mb.sp_rve_desc * 1)(*descs[:1])
+    assert mb.lib().sp_batch_create(0, arr, None, C.byref(h)) == mb.SP_ERR_ARG
+
+
+def test_large_rve_size_independent_properties():
+    """A 40^3 RVE (206,763 dof), too large for the CPU oracle in a test:
+    the stencil and assembled operators agree, the tangent is symmetric
+    (major symmetry of the homogenized stiffness), its diagonal is positive,
+    and the periodic tangent is bounded by it (Hill)."""
+    d = make_descs(40, [40])[0]
+    a, _, ia = mb.Batch([d]).homogenize()
+    b, _, ib = mb.Batch([d], op=mb.SP_OP_ELL).homogenize()
+    p, _, ip = mb.Batch([d], bc=mb.SP_BC_PERIODIC).homogenize()
+    for inf in (ia, ib, ip):
+        assert (mb.info_array(inf)["status"] == 0).all()
+    Ca, Cb, Cp = a[0].T, b[0].T, p[0].T
+    scale = np.abs(Ca).max()
+    assert np.abs(Ca - Cb).max() <= 2e-8 * scale
+    assert np.abs(Ca - Ca.T).max() <= 1e-7 * scale
+    assert (np.diag(Ca) > 0).all()
+    dC = Ca - Cp
+    assert np.linalg.eigvalsh((dC + dC.T) / 2).min() >= -1e-7 * scale
