@@ -240,3 +240,18 @@ def test_large_rve_size_independent_properties():
     assert (np.diag(Ca) > 0).all()
     dC = Ca - Cp
     assert np.linalg.eigvalsh((dC + dC.T) / 2).min() >= -1e-7 * scale
+
+
+def test_larger_sizes_stencil_agrees_with_assembled():
+    """The bench's larger sizes and beyond (n = 16 ... 28) on the stencil at
+    both one-CTA-per-SM shapes give the assembled operator's tangent, which
+    is tested against the oracle."""
+    descs = make_descs(77, [16, 20, 24, 28, 20])
+    for threads in (1024, 512):
+        a, _, ia = mb.Batch(descs, threads=threads, ctas_per_sm=1).homogenize()
+        assert (mb.info_array(ia)["status"] == 0).all()
+        if threads == 1024:
+            b, _, ib = mb.Batch(descs, op=mb.SP_OP_ELL).homogenize()
+            assert (mb.info_array(ib)["status"] == 0).all()
+        for i in range(len(descs)):
+            assert np.abs(a[i] - b[i]).max() <= 2e-8 * np.abs(b[i]).max(), (threads, i)
