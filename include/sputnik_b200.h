@@ -248,6 +248,9 @@ typedef struct {
   int idle_spin_limit;  /* empty polls before the loop returns (0: default) */
   int op;               /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int ctas_per_sm;      /* request slots per SM: 1 or 2 (0: 1 for the stencil, 2 for ELL) */
+  double refine_rtol;   /* a request whose warm-start prediction misses rtol is solved to
+                           this tighter tolerance, so that predictions from its solutions
+                           meet rtol without a solve (0: rtol / 100) */
 } sp_server_opts;
 
 void sp_server_opts_default(sp_server_opts *o);

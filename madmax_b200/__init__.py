@@ -72,7 +72,8 @@ class sp_batch_opts(C.Structure):
 class sp_server_opts(C.Structure):
     _fields_ = [("hbm_budget", C.c_size_t), ("max_inflight", C.c_int),
                 ("queue_capacity", C.c_int), ("rtol", C.c_double), ("inner_rtol", C.c_double),
-                ("idle_spin_limit", C.c_int), ("op", C.c_int), ("ctas_per_sm", C.c_int)]
+                ("idle_spin_limit", C.c_int), ("op", C.c_int), ("ctas_per_sm", C.c_int),
+                ("refine_rtol", C.c_double)]
 
 
 SP_ACTION_NULL, SP_ACTION_MICRO_CALC_STRESS, SP_ACTION_MICRO_CALC_C_TANGENT = 0, 1, 2

@@ -58,6 +58,9 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   constexpr bool PER = OP == SP_OP_STENCIL_PER;
   constexpr bool STENCIL = OP == SP_OP_STENCIL || PER;
   __shared__ double sKe[2 * SP_KE];
+  // FP64 stencil tables for the residual (an FP64 stencil batch has them in sKeT already)
+  constexpr bool OWN_KBD = !PER && !(STENCIL && sizeof(T) == 8);
+  __shared__ __align__(16) double sKBd[OWN_KBD ? SP_KB_SIZE : 2];
   // element scatter values (assembled operator) or element blocks (stencil)
   __shared__ __align__(16) T sKeT[STENCIL ? SP_KB_SIZE : 2 * SP_KE];
   __shared__ double sD[72], sBbar[144], sdsh[192];
@@ -111,6 +114,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     __syncthreads();
     elem_ops_stage2(t, NT, h, sdsh, sD, 2, sKe, sBbar);
     __syncthreads();
+    if constexpr (OWN_KBD) stencil_blocks<double>(t, NT, sKe, sKBd);
     T *nsv = nullptr, *dinv;
     if constexpr (STENCIL) {
       // 2s. no assembly: the stencil block tables and the Jacobi diagonal
@@ -152,6 +156,9 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     SolveArgs sa;
     sa.nrhs = P.nrhs;
     sa.rtol = P.rtol;
+    sa.rtol_refine = P.rtol;
+    sa.rn0_given = nullptr;
+    sa.kbd = PER ? nullptr : (OWN_KBD ? sKBd : reinterpret_cast<const double *>(sKeT));
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;

@@ -33,6 +33,12 @@ struct SolveArgs {
   double rtol, inner_rtol;
   int max_outer, max_inner;
   int warm;  // u's interior holds a start iterate other than 0
+  double rtol_refine;  // target once a refinement step has run (<= rtol): a start
+                       // iterate that already meets rtol is accepted as it is
+  const double *rn0_given;  // warm start: the right-hand sides' norms [K] when the
+                            // caller knows them (else one boundary-only residual)
+  const double *kbd;  // FP64 stencil tables in shared memory (stencil_blocks<double>):
+                      // the Dirichlet residual in stencil form; null: element form
   const double *eps;  // periodic conditions: [K][6] strains of the load cases (shared)
 };
 
@@ -171,7 +177,16 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
   if (t == 0) sh->phase = 0;
   int outer = 0, inner = 0;
   rve_sync<CL>();
-  if (P.warm) {
+  if (P.warm && P.rn0_given) {
+    if (t < K) sh->rn0[t] = (t < P.nrhs) ? P.rn0_given[t] : 0.0;
+    __syncthreads();
+    for (int k = 0; k < P.nrhs; k++) {
+      if (sh->rn0[k] > 0.0) continue;
+      for (int idx = gt; idx < blk; idx += GNT)
+        if (idx % g.nn_pad < g.nn && !is_bnode(g, idx % g.nn_pad)) u[(size_t)k * blk + idx] = 0.0;
+    }
+    rve_sync<CL>();
+  } else if (P.warm) {
     // The stopping rule is relative to the right-hand side, the residual of
     // the boundary values alone (not to the residual of the start iterate,
     // which a good warm start makes tiny).  A load case whose right-hand
@@ -209,6 +224,11 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
           residual_per<K, T, true>(gt, GNT, g, etype, sKe, P.eps, u, r, m1, m1 + K);
         else
           residual_per<K, T>(gt, GNT, g, etype, sKe, P.eps, u, r, m1);
+      } else if (P.kbd) {
+        if (first)
+          residual_stencil<K, T, true>(gt, GNT, g, etype, P.kbd, u, r, m1, m1 + K);
+        else
+          residual_stencil<K, T>(gt, GNT, g, etype, P.kbd, u, r, m1);
       } else {
         if (first)
           residual_soa<K, T, false, true>(gt, GNT, g, etype, sKe, u, r, m1, m1 + K);
@@ -227,7 +247,8 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
           if (first) sh->rn0[lane] = (rn <= SP_RHS_FLOOR * sqrt(red[tot + K + lane])) ? 0.0 : rn;
           sh->rn[lane] = rn;
           double rn0 = sh->rn0[lane];
-          notdone = lane < P.nrhs && rn0 > 0.0 && rn > P.rtol * rn0;
+          const double target = (outer == 0) ? P.rtol : P.rtol_refine;
+          notdone = lane < P.nrhs && rn0 > 0.0 && rn > target * rn0;
           sh->act[lane] = notdone;
         }
         unsigned b = __ballot_sync(0xffffffffu, notdone);

@@ -55,6 +55,7 @@ struct ServeGeom {
   double *Bbar; // [144]
   double *warm;     // [SERVE_K][3][nn_pad] solutions of the previous request
   double *warm_eps; // [SERVE_K][6] its load-case strains
+  double *gram;     // [6][6] b_i . b_j of the unit-strain right-hand sides b_i = -K u_bc(e_i)
   const int *color_elems;
   const uint8_t *slot;
   int color_off[9];
@@ -98,7 +99,7 @@ struct ServeParams {
   double *ws_u;
   float *ws_v;
   size_t stride;
-  double rtol, inner_rtol;
+  double rtol, inner_rtol, refine_rtol;
   int max_outer, max_inner, idle_limit;
 };
 
@@ -151,15 +152,64 @@ __global__ void __launch_bounds__(SERVE_NT) k_serve_assemble(ServeGeom *geoms, i
   }
 }
 
+// Gram matrix of every geometry's unit-strain right-hand sides: the right-
+// hand side of a strain eps is linear in it, b(eps) = sum_i eps_i b_i, so its
+// norm is sqrt(eps^T G eps) without a residual pass.  scratch: per CTA two
+// [6][3][max nn_pad] FP64 vectors.
+__global__ void __launch_bounds__(SERVE_NT) k_serve_gram(ServeGeom *geoms, int ngeom,
+                                                         double *scratch, size_t stride) {
+  __shared__ double sKe[2 * SP_KE];
+  __shared__ double seye[36];
+  __shared__ double red[33 * 21];
+  const int t = threadIdx.x;
+  double *u = scratch + (size_t)blockIdx.x * 2 * stride, *b = u + stride;
+  for (int i = t; i < 36; i += SERVE_NT) seye[i] = (i % 7 == 0) ? 1.0 : 0.0;
+  for (int gi = blockIdx.x; gi < ngeom; gi += gridDim.x) {
+    ServeGeom &G = geoms[gi];
+    const MeshGeo g = G.g;
+    for (int i = t; i < 2 * SP_KE; i += SERVE_NT) sKe[i] = G.Ke[i];
+    __syncthreads();
+    affine_soa<6>(t, SERVE_NT, g, seye, 6, false, u);
+    __syncthreads();
+    double nrm[6] = {0, 0, 0, 0, 0, 0};
+    residual_soa<6, double>(t, SERVE_NT, g, G.etype, sKe, u, b, nrm);
+    __syncthreads();
+    const size_t blk = (size_t)3 * g.nn_pad;
+    double acc[21];
+#pragma unroll
+    for (int q = 0; q < 21; q++) acc[q] = 0.0;
+    for (size_t i = t; i < blk; i += SERVE_NT) {
+      double v[6];
+#pragma unroll
+      for (int q = 0; q < 6; q++) v[q] = b[q * blk + i];
+      int q = 0;
+#pragma unroll
+      for (int a = 0; a < 6; a++)
+#pragma unroll
+        for (int c = a; c < 6; c++) acc[q++] += v[a] * v[c];
+    }
+    double tot[21];
+    block_sum<21>(acc, red, tot);
+    if (t == 0) {
+      int q = 0;
+      for (int a = 0; a < 6; a++)
+        for (int c = a; c < 6; c++, q++) G.gram[a * 6 + c] = G.gram[c * 6 + a] = tot[q];
+    }
+    __syncthreads();
+  }
+}
+
 template <int OP, int MINB>
 __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
   constexpr bool STENCIL = OP == SP_OP_STENCIL;
   __shared__ double sKe[2 * SP_KE], sD[72], sB[144];
   __shared__ __align__(16) float sKB[STENCIL ? SP_KB_SIZE : 4];
+  __shared__ __align__(16) double sKBd[SP_KB_SIZE];  // FP64 stencil tables (residual)
   __shared__ double red[33 * 16];
   __shared__ double savg[SP_MAX_RHS * 12];
   __shared__ double seps[SERVE_K * 6];
   __shared__ double spred[SERVE_K * 6];  // warm-start predictor coefficients
+  __shared__ double srn0[SERVE_K];       // right-hand-side norms from the Gram matrix
   __shared__ CgShared sh;
   __shared__ long long s_job;
   __shared__ int s_geom;
@@ -271,6 +321,13 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     // every load case inside; eps . x on the boundary (below)
     const size_t nu = (size_t)SERVE_K * 3 * g.nn_pad;
     const bool warm = *(volatile int *)&G.has_warm;
+    if (t < SERVE_K) {
+      // ||b(eps_k)||^2 = eps_k^T G eps_k
+      double s = 0.0;
+      for (int a = 0; a < 6; a++)
+        for (int c = 0; c < 6; c++) s += seps[t * 6 + a] * __ldg(G.gram + a * 6 + c) * seps[t * 6 + c];
+      srn0[t] = sqrt(fmax(s, 0.0));
+    }
     if (warm) {
       if (t < SERVE_K * 6) {
         const int k = t / 6, j = t % 6;
@@ -296,15 +353,21 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     }
     __syncthreads();
     if constexpr (STENCIL) stencil_blocks<float>(t, SERVE_NT, sKe, sKB);
+    stencil_blocks<double>(t, SERVE_NT, sKe, sKBd);
     affine_soa<SERVE_K>(t, SERVE_NT, g, seps, SERVE_NRHS, warm, u);
     __syncthreads();
     SolveArgs sa;
     sa.nrhs = SERVE_NRHS;
     sa.rtol = P.rtol;
+    // a request whose prediction misses rtol is solved tighter, so that the
+    // predictions from its solutions meet rtol without a solve
+    sa.rtol_refine = P.refine_rtol;
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
     sa.warm = warm;
+    sa.rn0_given = srn0;
+    sa.kbd = sKBd;
     sa.eps = nullptr;  // affine conditions: eps is carried by u's boundary values
     sp_solve_info in;
     if constexpr (STENCIL) {
@@ -316,13 +379,19 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
       in = solve_rve<float, SERVE_K, SERVE_NT, 1>(g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p,
                                                   q, sa, red, &sh, savg);
     }
-    // keep this request's solutions and strains as the geometry's next warm start
-    for (size_t i = t; i < nu; i += SERVE_NT) __stcg(G.warm + i, u[i]);
-    if (t < SERVE_K * 6) __stcg(G.warm_eps + t, seps[t]);
+    // keep this request's solutions and strains as the geometry's next warm
+    // start when it ran a refinement step (they then meet refine_rtol); a
+    // request accepted on its prediction leaves the solved state in place,
+    // so predictions do not drift from it
+    const bool store = in.outer_its > 0 || !warm;
+    if (store) {
+      for (size_t i = t; i < nu; i += SERVE_NT) __stcg(G.warm + i, u[i]);
+      if (t < SERVE_K * 6) __stcg(G.warm_eps + t, seps[t]);
+    }
     __threadfence();
     __syncthreads();
     if (t == 0) {
-      G.has_warm = 1;
+      if (store) G.has_warm = 1;
       for (int v = 0; v < 6; v++) out->stress[v] = savg[6 + v];
       // c_tangent[j*6 + i] = (stress(eps + d e_i)_j - stress(eps)_j) / (d e_i)
       // (micro/src/homogenize.c:79-80)
@@ -350,7 +419,7 @@ static size_t geom_bytes(const sp_rve_desc &d, int op) {
   size_t nn = (size_t)(d.n[0] + 1) * (d.n[1] + 1) * (d.n[2] + 1), np = (nn + 31) / 32 * 32;
   size_t nelm = (size_t)d.n[0] * d.n[1] * d.n[2];
   return (op == SP_OP_ELL ? np * 243 * 4 : 0) + 3 * np * 4 + nelm +
-         (2 * SP_KE + 72 + 144) * 8 + SERVE_K * (3 * np + 6) * 8 + 1024;
+         (2 * SP_KE + 72 + 144) * 8 + (SERVE_K * (3 * np + 6) + 36) * 8 + 1024;
 }
 
 }  // namespace sp
@@ -395,6 +464,7 @@ extern "C" void sp_server_opts_default(sp_server_opts *o) {
   o->idle_spin_limit = 2000000;
   o->op = SP_OP_STENCIL;
   o->ctas_per_sm = 0;
+  o->refine_rtol = 0.0;
 }
 
 static int server_layout(int ngeom, const sp_rve_desc *descs, const sp_server_opts *o, int nsm,
@@ -468,6 +538,8 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   if (o.queue_capacity <= 0) o.queue_capacity = 65536;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
   if (!(o.inner_rtol > 0)) o.inner_rtol = 1e-4;
+  if (!(o.refine_rtol > 0)) o.refine_rtol = 1e-2 * o.rtol;
+  if (o.refine_rtol > o.rtol) o.refine_rtol = o.rtol;
   if (o.idle_spin_limit <= 0) o.idle_spin_limit = 2000000;
   if (o.op != SP_OP_ELL && o.op != SP_OP_STENCIL)
     return sp_set_error(SP_ERR_ARG, "sp_server_create: unknown operator");
@@ -517,7 +589,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
     size_t np = G.g.nn_pad, ne = G.g.nelm;
     void *b[7] = {};
     size_t sz[7] = {o.op == SP_OP_ELL ? np * 243 * 4 : 0, 3 * np * 4, ne + 16, 2 * SP_KE * 8,
-                    72 * 8, 144 * 8, SERVE_K * (3 * np + 6) * 8};
+                    72 * 8, 144 * 8, (SERVE_K * (3 * np + 6) + 36) * 8};
     for (int k = 0; k < 7 && !rc; k++) {
       if (!sz[k]) continue;
       rc = dmalloc(&b[k], sz[k], &s->bytes);
@@ -532,6 +604,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
     G.Bbar = (double *)b[5];
     G.warm = (double *)b[6];
     G.warm_eps = G.warm + (size_t)SERVE_K * 3 * np;
+    G.gram = G.warm_eps + SERVE_K * 6;
     std::vector<uint8_t> et(ne);
     rc = sp_classify_elements(&dd, et.data(), nullptr);
     if (!rc && cudaMemcpy((void *)G.etype, et.data(), ne, cudaMemcpyHostToDevice))
@@ -582,6 +655,19 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
     if (cudaGetLastError() || cudaStreamSynchronize(s->stream))
       rc = sp_set_error(SP_ERR_CUDA, "geometry assembly failed");
   }
+  if (!rc) {
+    // Gram matrices of the unit-strain right-hand sides (temporary work space)
+    const int ngram = std::min(ngeom, 64);
+    const size_t gstride = (size_t)6 * 3 * maxnp;
+    double *d_gs = nullptr;
+    rc = dmalloc((void **)&d_gs, (size_t)ngram * 2 * gstride * sizeof(double), nullptr);
+    if (!rc) {
+      k_serve_gram<<<ngram, SERVE_NT, 0, s->stream>>>(s->d_geoms, ngeom, d_gs, gstride);
+      if (cudaGetLastError() || cudaStreamSynchronize(s->stream))
+        rc = sp_set_error(SP_ERR_CUDA, "geometry right-hand-side norms failed");
+    }
+    cudaFree(d_gs);
+  }
   cudaFree(d_mats);
   cudaFree(d_scr);
   if (rc) {
@@ -601,6 +687,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   P.ws_v = s->ws_v;
   P.stride = s->stride;
   P.rtol = o.rtol;
+  P.refine_rtol = o.refine_rtol;
   P.inner_rtol = o.inner_rtol;
   P.max_outer = 8;
   P.max_inner = 4000;
