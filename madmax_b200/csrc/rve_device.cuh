@@ -742,10 +742,13 @@ struct StencilAcc<float, K> {
 #pragma unroll
       for (int p = 0; p < KP; p++) v[d][p] = make_float2(0.f, 0.f);
   }
-  // v[d][q] += bv(d, c) x[q][c][nb]
-  __device__ void fma_block(const float *bv, const float *x, size_t blk, int nn_pad, int nb) {
+  // v[d][q] += bv(d, c) x[q][c][nb] for the pairs of load cases with an
+  // active case (bit q of amask; warp-uniform)
+  __device__ void fma_block(const float *bv, const float *x, size_t blk, int nn_pad, int nb,
+                            unsigned amask) {
 #pragma unroll
     for (int p = 0; p < KP; p++) {
+      if (!((amask >> (2 * p)) & 3u)) continue;
       float2 xb[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
@@ -773,9 +776,11 @@ struct StencilAcc<double, K> {
 #pragma unroll
       for (int q = 0; q < K; q++) v[d][q] = 0.0;
   }
-  __device__ void fma_block(const double *bv, const double *x, size_t blk, int nn_pad, int nb) {
+  __device__ void fma_block(const double *bv, const double *x, size_t blk, int nn_pad, int nb,
+                            unsigned amask) {
 #pragma unroll
     for (int q = 0; q < K; q++) {
+      if (!((amask >> q) & 1u)) continue;
       double xb[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) xb[c] = x[q * blk + (size_t)c * nn_pad + nb];
@@ -796,11 +801,12 @@ struct StencilAcc<double, K> {
 // lie inside one material reads that material's assembled blocks (one
 // shared-memory broadcast per load); other warps sum each neighbour block
 // from the element blocks of their own materials.  Adds x.y per load case
-// into dot[K].
+// into dot[K].  Load cases whose bit in amask is clear (converged; uniform
+// across the block) are neither read nor written.
 template <typename T, int K, bool PER = false>
 __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB,
                                     const uint8_t *__restrict__ etype, const T *x, T *y,
-                                    double *dot) {
+                                    double *dot, unsigned amask = ~0u) {
   using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
   const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
   const int mx = PER ? g.nex : g.nx - 2, my = PER ? g.ney : g.ny - 2, mz = PER ? g.nez : g.nz - 2;
@@ -861,7 +867,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
           const int dx = mm % 3 - 1, dy = mm / 3 - 1;
           A bv[9] = {};
           add_block<T, A>(ka + ((dz + 1) * 9 + mm) * SP_KB_BLK, bv);
-          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz));
+          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz), amask);
         }
       }
     } else {
@@ -885,13 +891,14 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
             const int lb = hex8_local(bx, by, 0) + 4 * bz;
             add_block<T, A>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK, bv);
           }
-          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz));
+          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz), amask);
         }
       }
     }
     if (valid) {
 #pragma unroll
-      for (int q = 0; q < K; q++)
+      for (int q = 0; q < K; q++) {
+        if (!((amask >> q) & 1u)) continue;
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           size_t o = q * blk + (size_t)d * g.nn_pad + a;
@@ -899,6 +906,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
           dot[q] += (double)yv * (double)x[o];
           y[o] = yv;
         }
+      }
     }
   }
 }

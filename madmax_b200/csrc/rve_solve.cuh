@@ -47,6 +47,7 @@ struct CgShared {
   double alpha[SP_MAX_RHS], beta[SP_MAX_RHS];
   int act[SP_MAX_RHS];
   int nact, done;
+  unsigned amask;  // bit k: load case k still active in the inner CG
   // cluster reduction: [buffer][rank][value], written by every rank into
   // rank 0's copy
   double cpart[2][8][16];
@@ -120,7 +121,8 @@ template <typename T, int K>
 struct EllOp {
   const T *nsv;
   const int *nbr;
-  __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot) const {
+  __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
+                        unsigned) const {
     spmm_ns<T, K, false>(gt, gnt, g, nsv, nbr, p, q, dot);
   }
 };
@@ -129,8 +131,9 @@ template <typename T, int K, bool PER = false>
 struct StencilOp {
   const T *kb;  // shared-memory element blocks (stencil_blocks)
   const uint8_t *etype;
-  __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot) const {
-    spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot);
+  __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
+                        unsigned amask) const {
+    spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask);
   }
 };
 
@@ -292,7 +295,10 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
           sh->act[lane] = a;
         }
         unsigned b = __ballot_sync(0xffffffffu, a);
-        if (lane == 0) sh->nact = __popc(b);
+        if (lane == 0) {
+          sh->nact = __popc(b);
+          sh->amask = b;
+        }
       }
       __syncthreads();
     }
@@ -304,7 +310,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         double m3[K];
 #pragma unroll
         for (int k = 0; k < K; k++) m3[k] = 0.0;
-        op.apply(gt, GNT, g, p, q, m3);
+        op.apply(gt, GNT, g, p, q, m3, sh->amask);
         rve_reduce<K, CL>(m3, red, sh);
         if (warp == 0 && lane < K) {
           double pq = red[32 * K + lane];
@@ -322,10 +328,12 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         T al[K];
 #pragma unroll
         for (int k = 0; k < K; k++) al[k] = (T)sh->alpha[k];
+        const unsigned am = sh->amask;  // converged load cases are left as they are
         for (int c = gt; c < nch; c += GNT) {
           const W dv = W::load(dinv + (size_t)c * E);
 #pragma unroll
           for (int k = 0; k < K; k++) {
+            if (!((am >> k) & 1u)) continue;
             const size_t o = (size_t)k * blk + (size_t)c * E;
             W xv = W::load(x + o), pv = W::load(p + o), rv = W::load(r + o), qv = W::load(q + o);
 #pragma unroll
@@ -351,7 +359,10 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
             sh->act[lane] = a;
           }
           unsigned b = __ballot_sync(0xffffffffu, a);
-          if (lane == 0) sh->nact = __popc(b);
+          if (lane == 0) {
+            sh->nact = __popc(b);
+            sh->amask = b;
+          }
         }
         __syncthreads();
       }
@@ -362,10 +373,12 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         T be[K];
 #pragma unroll
         for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
+        const unsigned am = sh->amask;
         for (int c = gt; c < nch; c += GNT) {
           const W dv = W::load(dinv + (size_t)c * E);
 #pragma unroll
           for (int k = 0; k < K; k++) {
+            if (!((am >> k) & 1u)) continue;
             const size_t o = (size_t)k * blk + (size_t)c * E;
             W rv = W::load(r + o), pv = W::load(p + o);
 #pragma unroll
