@@ -191,7 +191,7 @@ typedef struct {
   int nrhs;          /* load cases per RVE, 1..8 (default 6) */
   int precision;     /* SP_PREC_MIXED (default) or SP_PREC_FP64 */
   double rtol;       /* FP64 residual target per rhs (default 1e-8) */
-  double inner_rtol; /* FP32 CG reduction per refinement step (default 1e-4) */
+  double inner_rtol; /* CG residual reduction per refinement step (default 1e-4) */
   int max_outer;     /* refinement steps (default 8) */
   int max_inner;     /* CG iterations per step (default 4000) */
   int threads;       /* threads per CTA (0: 1024 for the stencil, 512 otherwise) */
@@ -244,7 +244,7 @@ typedef struct {
   int max_inflight;     /* request slots solving at once (0: one per CTA) */
   int queue_capacity;   /* request ring size (0: 65536) */
   double rtol;          /* default 1e-8 */
-  double inner_rtol;    /* default 1e-4 */
+  double inner_rtol;    /* CG residual reduction per refinement step (default 1e-4) */
   int idle_spin_limit;  /* empty polls before the loop returns (0: default) */
   int op;               /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int ctas_per_sm;      /* request slots per SM: 1 or 2 (0: 1 for the stencil, 2 for ELL) */

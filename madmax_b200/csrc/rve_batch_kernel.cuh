@@ -198,7 +198,8 @@ using BatchFn = void (*)(BatchParams);
   X(T, K, 512, 2, 8, SP_OP_ELL) \
   X(T, K, 512, 1, 1, SP_OP_STENCIL) X(T, K, 512, 2, 1, SP_OP_STENCIL) \
   X(T, K, 256, 2, 1, SP_OP_STENCIL) X(T, K, 256, 4, 1, SP_OP_STENCIL) \
-  X(T, K, 1024, 1, 1, SP_OP_STENCIL) \
+  X(T, K, 1024, 1, 1, SP_OP_STENCIL) X(T, K, 1024, 1, 2, SP_OP_STENCIL) \
+  X(T, K, 1024, 1, 4, SP_OP_STENCIL) X(T, K, 1024, 1, 8, SP_OP_STENCIL) \
   X(T, K, 512, 1, 1, SP_OP_STENCIL_PER) X(T, K, 512, 2, 1, SP_OP_STENCIL_PER)
 #define SP_BATCH_SHAPES_FP64(X, T, K) \
   X(T, K, 512, 1, 1, SP_OP_ELL) X(T, K, 512, 2, 1, SP_OP_ELL) \

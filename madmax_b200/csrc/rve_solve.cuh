@@ -43,9 +43,11 @@ struct SolveArgs {
 };
 
 struct CgShared {
-  double rn0[SP_MAX_RHS], rn[SP_MAX_RHS], rho[SP_MAX_RHS], rr0[SP_MAX_RHS];
+  double rn0[SP_MAX_RHS], rn[SP_MAX_RHS], rho[SP_MAX_RHS];
   double alpha[SP_MAX_RHS], beta[SP_MAX_RHS];
+  double thr[SP_MAX_RHS];  // inner CG: r.r at which a load case's correction ends
   int act[SP_MAX_RHS];
+  int keep[SP_MAX_RHS];    // load case k continues the last correction's direction
   int nact, done;
   unsigned amask;  // bit k: load case k still active in the inner CG
   // cluster reduction: [buffer][rank][value], written by every rank into
@@ -176,6 +178,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
   if (t < SP_MAX_RHS) {
     sh->rn0[t] = 0.0;
     sh->act[t] = 0;
+    sh->keep[t] = 0;
   }
   if (t == 0) sh->phase = 0;
   int outer = 0, inner = 0;
@@ -212,6 +215,32 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
     }
     rve_sync<CL>();
   }
+  // p = D^-1 r + beta p for the active load cases, chunk-major: the diagonal
+  // is read once per chunk and the load cases' loads are independent
+  auto pdir = [&](unsigned am) {
+    T be[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
+    for (int c = gt; c < nch; c += GNT) {
+      const W dv = W::load(dinv + (size_t)c * E);
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        if (!((am >> k) & 1u)) continue;
+        const size_t o = (size_t)k * blk + (size_t)c * E;
+        const W rv = W::load(r + o);
+        W pv;
+        if (be[k] == T(0)) {  // a fresh start never reads p (the work space may hold anything)
+#pragma unroll
+          for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e];
+        } else {
+          pv = W::load(p + o);
+#pragma unroll
+          for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be[k] * pv.v[e];
+        }
+        pv.store(p + o);
+      }
+    }
+  };
   for (;;) {
     // 3a. FP64 residual b = -K u -> r (type T) and its norms; on a cold
     // start the first one is the right-hand side, whose norm the later
@@ -263,36 +292,48 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
       __syncthreads();
     }
     if (sh->done) break;
-    // 3b. Jacobi-PCG on A x = r in precision T: x = 0, p = z = D^-1 r
+    // 3b. Jacobi-PCG on A x = r in precision T with x = 0.  The search
+    // direction carries over from the previous correction (a reliable
+    // update: r is replaced by the true residual, the Krylov recurrence goes
+    // on), p = D^-1 r + beta p with beta = r.z / rho of the last step; the
+    // first correction, or a load case that sat out the last one, starts
+    // from p = D^-1 r.  A correction ends when r.r has fallen by inner_rtol^2
+    // or below the final target with a factor 2 margin.
     {
       double m2[2 * K];
 #pragma unroll
       for (int k = 0; k < 2 * K; k++) m2[k] = 0.0;
+      W zero;
 #pragma unroll
-      for (int k = 0; k < K; k++) {
-        for (int c = gt; c < nch; c += GNT) {
-          size_t o = (size_t)k * blk + (size_t)c * E;
-          W rv = W::load(r + o), dv = W::load(dinv + (size_t)c * E), zv, zero;
+      for (int e = 0; e < E; e++) zero.v[e] = T(0);
+      for (int c = gt; c < nch; c += GNT) {
+        const W dv = W::load(dinv + (size_t)c * E);
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+          const size_t o = (size_t)k * blk + (size_t)c * E;
+          const W rv = W::load(r + o);
 #pragma unroll
           for (int e = 0; e < E; e++) {
-            zv.v[e] = dv.v[e] * rv.v[e];
-            zero.v[e] = T(0);
-            m2[k] += (double)rv.v[e] * (double)zv.v[e];
+            m2[k] += (double)rv.v[e] * (double)(dv.v[e] * rv.v[e]);
             m2[K + k] += (double)rv.v[e] * (double)rv.v[e];
           }
-          zv.store(p + o);
           zero.store(x + o);
           zero.store(q + o);  // (entries an operator does not write stay 0)
         }
       }
-      rve_reduce<2 * K, CL>(m2, red, sh);  // (its cluster barrier also publishes p)
+      rve_reduce<2 * K, CL>(m2, red, sh);
       if (warp == 0) {
         bool a = false;
         if (lane < K) {
-          sh->rho[lane] = red[64 * K + lane];
-          sh->rr0[lane] = red[64 * K + K + lane];
-          a = sh->act[lane] && sh->rr0[lane] > 0.0;
+          const double rz = red[64 * K + lane], rr = red[64 * K + K + lane];
+          a = sh->act[lane] && rr > 0.0;
+          const double rho = sh->rho[lane];
+          sh->beta[lane] = (a && sh->keep[lane] && rho != 0.0) ? rz / rho : 0.0;
+          sh->rho[lane] = rz;
+          const double fin = 0.5 * P.rtol_refine * sh->rn0[lane];
+          sh->thr[lane] = fmax(P.inner_rtol * P.inner_rtol * rr, fin * fin);
           sh->act[lane] = a;
+          sh->keep[lane] = a;
         }
         unsigned b = __ballot_sync(0xffffffffu, a);
         if (lane == 0) {
@@ -301,8 +342,9 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         }
       }
       __syncthreads();
+      pdir(sh->amask);
+      rve_sync<CL>();  // the SpMM gathers p rows of every CTA
     }
-    const double tol2 = P.inner_rtol * P.inner_rtol;
     int it = 0;
     while (sh->nact > 0 && it < P.max_inner) {
       // q = A p, alpha = rho / p.q
@@ -352,7 +394,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
           bool a = false;
           if (lane < K) {
             double rz = red[64 * K + lane], rr = red[64 * K + K + lane];
-            a = sh->act[lane] && !(rr <= tol2 * sh->rr0[lane]);
+            a = sh->act[lane] && !(rr <= sh->thr[lane]);
             double rho = sh->rho[lane];
             sh->beta[lane] = (a && rho != 0.0) ? rz / rho : 0.0;
             if (a) sh->rho[lane] = rz;
@@ -368,25 +410,8 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
       }
       it++;
       if (sh->nact == 0) break;
-      // p = D^-1 r + beta p (chunk-major as above)
-      {
-        T be[K];
-#pragma unroll
-        for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
-        const unsigned am = sh->amask;
-        for (int c = gt; c < nch; c += GNT) {
-          const W dv = W::load(dinv + (size_t)c * E);
-#pragma unroll
-          for (int k = 0; k < K; k++) {
-            if (!((am >> k) & 1u)) continue;
-            const size_t o = (size_t)k * blk + (size_t)c * E;
-            W rv = W::load(r + o), pv = W::load(p + o);
-#pragma unroll
-            for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be[k] * pv.v[e];
-            pv.store(p + o);
-          }
-        }
-      }
+      // p = D^-1 r + beta p
+      pdir(sh->amask);
       rve_sync<CL>();  // the next SpMM gathers p rows of every CTA
     }
     inner += it;
