@@ -727,6 +727,18 @@ __device__ inline void add_block(const T *src, A *bv) {
   for (int u = 0; u < 9; u++) bv[u] += (A)w[u];
 }
 
+// Node-blocked layout of the stencil SpMM's input vector: the 3K streams
+// (component d, load case k) of 32 consecutive nodes lie next to each other,
+//   v[((node / 32) * 3K + d*K + k) * 32 + node % 32],
+// so the 3K values a lane gathers for one neighbour sit at compile-time
+// offsets from one address (one address computation per neighbour instead
+// of one per value).  A 16-byte chunk of 4 (FP32) or 2 (FP64) nodes of one
+// stream is contiguous in both this and the component-major layout.
+template <int K>
+__device__ __forceinline__ size_t nbk_base(int node) {
+  return (size_t)(node >> 5) * (96 * K) + (node & 31);
+}
+
 // Accumulators of the stencil SpMM: FP32 pairs of load cases updated with
 // the packed FP32x2 FMA, or FP64 scalars.
 template <typename T, int K>
@@ -742,25 +754,25 @@ struct StencilAcc<float, K> {
 #pragma unroll
       for (int p = 0; p < KP; p++) v[d][p] = make_float2(0.f, 0.f);
   }
-  // v[d][q] += bv(d, c) x[q][c][nb] for the pairs of load cases with an
-  // active case (bit q of amask; warp-uniform)
-  __device__ void fma_block(const float *bv, const float *x, size_t blk, int nn_pad, int nb,
-                            unsigned amask) {
+  // v[d][q] += bv(d, c) x(q, c), x(q, c) = xb[(c*K + q) * 32] (node-blocked),
+  // for the pairs of load cases with an active case (bit q of amask;
+  // warp-uniform)
+  __device__ void fma_block(const float *bv, const float *xb, unsigned amask) {
 #pragma unroll
     for (int p = 0; p < KP; p++) {
       if (!((amask >> (2 * p)) & 3u)) continue;
-      float2 xb[3];
+      float2 xv[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        xb[c].x = x[(2 * p) * blk + (size_t)c * nn_pad + nb];
-        xb[c].y = (2 * p + 1 < K) ? x[(2 * p + 1) * blk + (size_t)c * nn_pad + nb] : 0.f;
+        xv[c].x = xb[(c * K + 2 * p) * 32];
+        xv[c].y = (2 * p + 1 < K) ? xb[(c * K + 2 * p + 1) * 32] : 0.f;
       }
 #pragma unroll
       for (int d = 0; d < 3; d++)
 #pragma unroll
         for (int c = 0; c < 3; c++) {
           const float b = bv[d * 3 + c];
-          v[d][p] = __ffma2_rn(make_float2(b, b), xb[c], v[d][p]);
+          v[d][p] = __ffma2_rn(make_float2(b, b), xv[c], v[d][p]);
         }
     }
   }
@@ -776,24 +788,24 @@ struct StencilAcc<double, K> {
 #pragma unroll
       for (int q = 0; q < K; q++) v[d][q] = 0.0;
   }
-  __device__ void fma_block(const double *bv, const double *x, size_t blk, int nn_pad, int nb,
-                            unsigned amask) {
+  __device__ void fma_block(const double *bv, const double *xb, unsigned amask) {
 #pragma unroll
     for (int q = 0; q < K; q++) {
       if (!((amask >> q) & 1u)) continue;
-      double xb[3];
+      double xv[3];
 #pragma unroll
-      for (int c = 0; c < 3; c++) xb[c] = x[q * blk + (size_t)c * nn_pad + nb];
+      for (int c = 0; c < 3; c++) xv[c] = xb[(c * K + q) * 32];
 #pragma unroll
       for (int d = 0; d < 3; d++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) v[d][q] = fma(bv[d * 3 + c], xb[c], v[d][q]);
+        for (int c = 0; c < 3; c++) v[d][q] = fma(bv[d * 3 + c], xv[c], v[d][q]);
     }
   }
   __device__ double get(int d, int q) const { return v[d][q]; }
 };
 
-// y = A x (K right-hand sides, component-major) with the stencil operator.
+// y = A x (K right-hand sides; x node-blocked (nbk_base), y component-major)
+// with the stencil operator.
 // Dirichlet (PER = false): interior nodes only; boundary and padding entries
 // of y are not written.  Periodic (PER): every node of the periodic grid,
 // neighbours and elements wrapped, y = 0 at the fixed node 0.  A warp takes
@@ -867,7 +879,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
           const int dx = mm % 3 - 1, dy = mm / 3 - 1;
           A bv[9] = {};
           add_block<T, A>(ka + ((dz + 1) * 9 + mm) * SP_KB_BLK, bv);
-          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz), amask);
+          acc.fma_block(bv, x + nbk_base<K>(nbr_of(dx, dy, dz)), amask);
         }
       }
     } else {
@@ -891,7 +903,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
             const int lb = hex8_local(bx, by, 0) + 4 * bz;
             add_block<T, A>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK, bv);
           }
-          acc.fma_block(bv, x, blk, g.nn_pad, nbr_of(dx, dy, dz), amask);
+          acc.fma_block(bv, x + nbk_base<K>(nbr_of(dx, dy, dz)), amask);
         }
       }
     }
@@ -901,10 +913,9 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
         if (!((amask >> q) & 1u)) continue;
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-          size_t o = q * blk + (size_t)d * g.nn_pad + a;
           T yv = (PER && a == 0) ? T(0) : (T)acc.get(d, q);
-          dot[q] += (double)yv * (double)x[o];
-          y[o] = yv;
+          dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
+          y[q * blk + (size_t)d * g.nn_pad + a] = yv;
         }
       }
     }

@@ -121,6 +121,7 @@ __device__ inline void rve_reduce(const double *v, double *red, CgShared *sh) {
 // memory).  apply() computes q = A p and adds p.q per load case into dot.
 template <typename T, int K>
 struct EllOp {
+  static constexpr bool kBlocked = false;  // p component-major
   const T *nsv;
   const int *nbr;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
@@ -131,6 +132,7 @@ struct EllOp {
 
 template <typename T, int K, bool PER = false>
 struct StencilOp {
+  static constexpr bool kBlocked = true;  // p node-blocked (nbk_base)
   const T *kb;  // shared-memory element blocks (stencil_blocks)
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
@@ -215,6 +217,20 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
     }
     rve_sync<CL>();
   }
+  // The vector passes walk 16-byte chunks in node order: chunk c covers E
+  // nodes of stream segment sg = c / CPB (32 nodes of component d), whose
+  // offset is cm(c) + k*blk for load case k in the component-major vectors
+  // and pb(c) + k*32 in a node-blocked p (the stencil operator's input).
+  constexpr int CPB = 32 / E;
+  auto cm = [&](int c) -> size_t {
+    const int sg = c / CPB, b = sg / 3, d = sg - 3 * b;
+    return (size_t)d * g.nn_pad + b * 32 + (c - sg * CPB) * E;
+  };
+  auto pb = [&](int c) -> size_t {
+    const int sg = c / CPB;
+    return Op::kBlocked ? (size_t)sg * (32 * K) + (c - sg * CPB) * E : cm(c);
+  };
+  const size_t pk = Op::kBlocked ? 32 : blk;  // p offset between load cases
   // p = D^-1 r + beta p for the active load cases, chunk-major: the diagonal
   // is read once per chunk and the load cases' loads are independent
   auto pdir = [&](unsigned am) {
@@ -222,22 +238,23 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
 #pragma unroll
     for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
     for (int c = gt; c < nch; c += GNT) {
-      const W dv = W::load(dinv + (size_t)c * E);
+      const size_t oc = cm(c), op_ = pb(c);
+      const W dv = W::load(dinv + oc);
 #pragma unroll
       for (int k = 0; k < K; k++) {
         if (!((am >> k) & 1u)) continue;
-        const size_t o = (size_t)k * blk + (size_t)c * E;
+        const size_t o = (size_t)k * blk + oc, opk = op_ + k * pk;
         const W rv = W::load(r + o);
         W pv;
         if (be[k] == T(0)) {  // a fresh start never reads p (the work space may hold anything)
 #pragma unroll
           for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e];
         } else {
-          pv = W::load(p + o);
+          pv = W::load(p + opk);
 #pragma unroll
           for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be[k] * pv.v[e];
         }
-        pv.store(p + o);
+        pv.store(p + opk);
       }
     }
   };
@@ -372,12 +389,14 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         for (int k = 0; k < K; k++) al[k] = (T)sh->alpha[k];
         const unsigned am = sh->amask;  // converged load cases are left as they are
         for (int c = gt; c < nch; c += GNT) {
-          const W dv = W::load(dinv + (size_t)c * E);
+          const size_t oc = cm(c), op_ = pb(c);
+          const W dv = W::load(dinv + oc);
 #pragma unroll
           for (int k = 0; k < K; k++) {
             if (!((am >> k) & 1u)) continue;
-            const size_t o = (size_t)k * blk + (size_t)c * E;
-            W xv = W::load(x + o), pv = W::load(p + o), rv = W::load(r + o), qv = W::load(q + o);
+            const size_t o = (size_t)k * blk + oc;
+            W xv = W::load(x + o), pv = W::load(p + op_ + k * pk), rv = W::load(r + o),
+              qv = W::load(q + o);
 #pragma unroll
             for (int e = 0; e < E; e++) {
               xv.v[e] += al[k] * pv.v[e];
