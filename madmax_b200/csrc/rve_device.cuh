@@ -814,11 +814,12 @@ struct StencilAcc<double, K> {
 // shared-memory broadcast per load); other warps sum each neighbour block
 // from the element blocks of their own materials.  Adds x.y per load case
 // into dot[K].  Load cases whose bit in amask is clear (converged; uniform
-// across the block) are neither read nor written.
+// across the block) are neither read nor written.  rev: the warps walk the
+// node groups from the last to the first.
 template <typename T, int K, bool PER = false>
 __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB,
                                     const uint8_t *__restrict__ etype, const T *x, T *y,
-                                    double *dot, unsigned amask = ~0u) {
+                                    double *dot, unsigned amask = ~0u, bool rev = false) {
   using A = typename std::conditional<sizeof(T) == 4, float, double>::type;
   const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
   const int mx = PER ? g.nex : g.nx - 2, my = PER ? g.ney : g.ny - 2, mz = PER ? g.nez : g.nz - 2;
@@ -827,7 +828,9 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
   const int sy = PER ? g.nex : g.nx, sz = PER ? g.nex * g.ney : g.nx * g.ny;
   const int esy = g.nex, esz = g.nex * g.ney;
   const size_t blk = (size_t)3 * g.nn_pad;
-  for (int s0 = warp * 32; s0 < ni; s0 += nwarps * 32) {
+  const int ngr = (ni + 31) / 32;
+  for (int gi = warp; gi < ngr; gi += nwarps) {
+    const int s0 = (rev ? ngr - 1 - gi : gi) * 32;
     const int id = s0 + lane;
     const bool valid = id < ni;
     const int idc = valid ? id : ni - 1;
@@ -914,6 +917,137 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           T yv = (PER && a == 0) ? T(0) : (T)acc.get(d, q);
+          dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
+          y[q * blk + (size_t)d * g.nn_pad + a] = yv;
+        }
+      }
+    }
+  }
+}
+
+// FP32 stencil SpMM under Dirichlet conditions with the x-neighbours taken
+// from the warp.  A warp holds 32 consecutive interior nodes: lanes 1..30
+// produce output, lanes 0 and 31 only supply values.  For each of the 9
+// (dy, dz) neighbour rows a lane loads the 3K values of its own column
+// (dx = 0, one gather); the dx = -1 / +1 values come from the adjacent
+// lanes (shuffles), or are 0 where that neighbour is a boundary node (the
+// CG vectors vanish on the Dirichlet boundary) -- exactly the case in which
+// the adjacent lane holds a node of another row.  9 instead of 27 gathers
+// per value; the blocks, materials and output are those of spmm_stencil.
+template <int K>
+__device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const float *KB,
+                                       const uint8_t *__restrict__ etype, const float *x,
+                                       float *y, double *dot, unsigned amask, bool rev) {
+  constexpr int KP = (K + 1) / 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
+  const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
+  const int ni = mx * my * mz;
+  const int sy = g.nx, sz = g.nx * g.ny;
+  const int esy = g.nex, esz = g.nex * g.ney;
+  const size_t blk = (size_t)3 * g.nn_pad;
+  const int ngr = (ni + 29) / 30;
+  for (int gi = warp; gi < ngr; gi += nwarps) {
+    const int s0 = (rev ? ngr - 1 - gi : gi) * 30;
+    const int id = s0 - 1 + lane;
+    const bool out = lane >= 1 && lane <= 30 && id < ni;
+    const int idc = min(max(id, 0), ni - 1);
+    const int ii = idc % mx, jj = (idc / mx) % my, kk = idc / (mx * my);
+    const int i = ii + 1, j = jj + 1, k = kk + 1;
+    const int a = i + j * sy + k * sz;
+    // the adjacent lanes hold the x-neighbours unless those are boundary nodes
+    const bool lo = ii > 0, hi = ii < mx - 1;
+    int tb[8];  // offset of the element's material blocks in KB
+    unsigned mask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+      const int e = (i - 1 + ox) + (j - 1 + oy) * esy + (k - 1 + oz) * esz;
+      const unsigned te = __ldg(etype + e);
+      mask |= te << c;
+      tb[c] = SP_KE_OFF + (int)te * SP_KB_TYPE;
+    }
+    const bool all0 = __all_sync(FULL, !out || mask == 0u);
+    const bool all1 = __all_sync(FULL, !out || mask == 0xffu);
+    const bool pure = all0 || all1;
+    const float *ka = KB + SP_KA_OFF + (all1 ? 27 * SP_KB_BLK : 0);
+    float2 acc[3][KP];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int p = 0; p < KP; p++) acc[d][p] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int dz = -1; dz <= 1; dz++) {
+#pragma unroll
+      for (int dy = -1; dy <= 1; dy++) {
+        const float *xb = x + nbk_base<K>(a + dy * sy + dz * sz);
+        float2 xv[3][KP];
+#pragma unroll
+        for (int p = 0; p < KP; p++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            xv[c][p] = make_float2(0.f, 0.f);
+            if ((amask >> (2 * p)) & 3u) {
+              xv[c][p].x = xb[(c * K + 2 * p) * 32];
+              if (2 * p + 1 < K) xv[c][p].y = xb[(c * K + 2 * p + 1) * 32];
+            }
+          }
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+          float bv[9] = {};
+          if (pure) {
+            add_block<float, float>(ka + ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) * SP_KB_BLK, bv);
+          } else {
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+              const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+              const int bx = 1 - ox + dx, by = 1 - oy + dy;
+              if (bx < 0 || bx > 1 || by < 0 || by > 1) continue;  // resolved at compile time
+              const int bz = 1 - oz + dz;                            // warp-uniform
+              if (bz < 0 || bz > 1) continue;
+              const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+              const int lb = hex8_local(bx, by, 0) + 4 * bz;
+              add_block<float, float>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK, bv);
+            }
+          }
+#pragma unroll
+          for (int p = 0; p < KP; p++) {
+            if (!((amask >> (2 * p)) & 3u)) continue;
+            float2 xs[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              if (dx == 0) {
+                xs[c] = xv[c][p];
+              } else {
+                float2 v;
+                if (dx < 0) {
+                  v.x = __shfl_up_sync(FULL, xv[c][p].x, 1);
+                  v.y = __shfl_up_sync(FULL, xv[c][p].y, 1);
+                } else {
+                  v.x = __shfl_down_sync(FULL, xv[c][p].x, 1);
+                  v.y = __shfl_down_sync(FULL, xv[c][p].y, 1);
+                }
+                xs[c] = (dx < 0 ? lo : hi) ? v : make_float2(0.f, 0.f);
+              }
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                const float b = bv[d * 3 + c];
+                acc[d][p] = __ffma2_rn(make_float2(b, b), xs[c], acc[d][p]);
+              }
+          }
+        }
+      }
+    }
+    if (out) {
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        if (!((amask >> q) & 1u)) continue;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const float yv = (q & 1) ? acc[d][q >> 1].y : acc[d][q >> 1].x;
           dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
           y[q * blk + (size_t)d * g.nn_pad + a] = yv;
         }

@@ -125,7 +125,7 @@ struct EllOp {
   const T *nsv;
   const int *nbr;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
-                        unsigned) const {
+                        unsigned, bool) const {
     spmm_ns<T, K, false>(gt, gnt, g, nsv, nbr, p, q, dot);
   }
 };
@@ -136,8 +136,11 @@ struct StencilOp {
   const T *kb;  // shared-memory element blocks (stencil_blocks)
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
-                        unsigned amask) const {
-    spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask);
+                        unsigned amask, bool rev) const {
+    if constexpr (sizeof(T) == 4 && !PER && K <= 6)
+      spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+    else
+      spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
   }
 };
 
@@ -231,13 +234,19 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
     return Op::kBlocked ? (size_t)sg * (32 * K) + (c - sg * CPB) * E : cm(c);
   };
   const size_t pk = Op::kBlocked ? 32 : blk;  // p offset between load cases
+  // Consecutive passes over the vectors walk the nodes in opposite
+  // directions, so each pass starts on the lines the previous one touched
+  // last, which are still in L2.
+  int npass = 0;
   // p = D^-1 r + beta p for the active load cases, chunk-major: the diagonal
   // is read once per chunk and the load cases' loads are independent
   auto pdir = [&](unsigned am) {
     T be[K];
 #pragma unroll
     for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
-    for (int c = gt; c < nch; c += GNT) {
+    const bool rev = (npass++ & 1) != 0;
+    for (int c0 = gt; c0 < nch; c0 += GNT) {
+      const int c = rev ? nch - 1 - c0 : c0;
       const size_t oc = cm(c), op_ = pb(c);
       const W dv = W::load(dinv + oc);
 #pragma unroll
@@ -369,7 +378,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         double m3[K];
 #pragma unroll
         for (int k = 0; k < K; k++) m3[k] = 0.0;
-        op.apply(gt, GNT, g, p, q, m3, sh->amask);
+        op.apply(gt, GNT, g, p, q, m3, sh->amask, (npass++ & 1) != 0);
         rve_reduce<K, CL>(m3, red, sh);
         if (warp == 0 && lane < K) {
           double pq = red[32 * K + lane];
@@ -388,7 +397,9 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
 #pragma unroll
         for (int k = 0; k < K; k++) al[k] = (T)sh->alpha[k];
         const unsigned am = sh->amask;  // converged load cases are left as they are
-        for (int c = gt; c < nch; c += GNT) {
+        const bool rev = (npass++ & 1) != 0;
+        for (int c0 = gt; c0 < nch; c0 += GNT) {
+          const int c = rev ? nch - 1 - c0 : c0;
           const size_t oc = cm(c), op_ = pb(c);
           const W dv = W::load(dinv + oc);
 #pragma unroll
