@@ -98,7 +98,8 @@ def ptxas_report() -> str:
     out = []
     for log in sorted(glob.glob(os.path.join(BUILD, "*.cu.o.log"))):
         for line in open(log):
-            if "ptxas info" in line and ("registers" in line or "spill" in line or "Compiling" in line):
+            if ("ptxas info" in line and ("registers" in line or "Compiling" in line)) or \
+                    "bytes spill" in line:
                 out.append(line.rstrip())
     return "\n".join(out)
 

@@ -652,7 +652,10 @@ __host__ __device__ constexpr int hex8_local(int cx, int cy, int cz) {
 }
 
 constexpr int SP_KB_BLK = 12;                        // padded 3x3 block (16-byte rows for float)
-constexpr int SP_KB_TYPE = 64 * SP_KB_BLK;           // element blocks of one material
+// element blocks of one material, padded by 4 entries: the two materials'
+// blocks then start in different shared-memory banks, so a warp whose lanes
+// read the same block of both materials is served without bank conflicts
+constexpr int SP_KB_TYPE = 64 * SP_KB_BLK + 4;
 constexpr int SP_KA_OFF = 0;                         // KA[t][m]: 2 x 27 blocks
 constexpr int SP_KE_OFF = 2 * 27 * SP_KB_BLK;        // KE[t][la][lb]: 2 x 64 blocks
 constexpr int SP_KB_SIZE = SP_KE_OFF + 2 * SP_KB_TYPE;
@@ -666,8 +669,10 @@ template <typename T>
 __device__ inline void stencil_blocks(int t, int nt, const double *Ke /*[2][576]*/, T *KB) {
   for (int x = t; x < SP_KB_SIZE; x += nt) {
     double v = 0.0;
-    const int w = x % SP_KB_BLK;
-    if (w < 9) {
+    // entry w of block b within the KA part or within one material's KE part
+    const int r = x < SP_KE_OFF ? x : (x - SP_KE_OFF) % SP_KB_TYPE;
+    const int w = r % SP_KB_BLK;
+    if (w < 9 && r < 64 * SP_KB_BLK) {
       const int d = w / 3, cc = w % 3;
       if (x < SP_KE_OFF) {
         const int ty = x / (27 * SP_KB_BLK), m = (x / SP_KB_BLK) % 27;
@@ -680,7 +685,7 @@ __device__ inline void stencil_blocks(int t, int nt, const double *Ke /*[2][576]
           v += Ke[ty * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
         }
       } else {
-        const int r = x - SP_KE_OFF, ty = r / SP_KB_TYPE, b = (r % SP_KB_TYPE) / SP_KB_BLK;
+        const int ty = (x - SP_KE_OFF) / SP_KB_TYPE, b = r / SP_KB_BLK;
         const int la = b / 8, lb = b % 8;
         v = Ke[ty * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
       }
