@@ -77,6 +77,7 @@ using namespace sp;
 
 struct sp_batch_s {
   int nrve = 0, nrhs = 6, kp = 6, dev = -1, grid = 0, last_launches = 0;
+  int dyn_smem = 0;  // dynamic shared memory of the kernel (pattern table)
   sp_batch_opts o;
   std::vector<DevPlan *> plans;
   std::vector<sp_rve_desc> descs;
@@ -242,10 +243,31 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
                         "cluster %d, %s operator in this precision", o.threads, o.ctas_per_sm,
                         o.cluster, o.op == SP_OP_ELL ? "assembled" : "stencil");
     int g = d->nsm * o.ctas_per_sm;
+    b->dyn_smem = sp_batch_uses_ptable(o.precision == SP_PREC_MIXED, kp, kernel_op(o)) ? SP_PT_BYTES : 0;
+    if (fn && !rc && b->dyn_smem) {
+      if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               b->dyn_smem) != cudaSuccess) {
+        cudaGetLastError();
+        rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: %d bytes of dynamic shared memory refused",
+                          b->dyn_smem);
+      }
+    }
+    if (o.cluster == 1 && fn && !rc) {
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)fn, o.threads,
+                                                        b->dyn_smem) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: %d-thread CTAs cannot be resident",
+                          o.threads);
+      } else {
+        g = d->nsm * std::min(o.ctas_per_sm, nb);
+      }
+    }
     if (o.cluster > 1 && !rc) {
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(g);
       cfg.blockDim = dim3(o.threads);
+      cfg.dynamicSmemBytes = b->dyn_smem;
       cudaLaunchAttribute at;
       at.id = cudaLaunchAttributeClusterDimension;
       at.val.clusterDim.x = o.cluster;
@@ -374,11 +396,12 @@ extern "C" int sp_batch_launch(sp_batch *b, void *stream) {
   BatchFn fn = pick(b->o.precision, b->nrhs, sh);
   SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
   if (b->o.cluster == 1) {
-    fn<<<b->grid, b->o.threads, 0, s>>>(b->P);
+    fn<<<b->grid, b->o.threads, b->dyn_smem, s>>>(b->P);
   } else {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(b->grid);
     cfg.blockDim = dim3(b->o.threads);
+    cfg.dynamicSmemBytes = b->dyn_smem;
     cfg.stream = s;
     cudaLaunchAttribute at;
     at.id = cudaLaunchAttributeClusterDimension;

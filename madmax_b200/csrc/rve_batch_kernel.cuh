@@ -12,6 +12,13 @@ namespace sp {
 // periodic boundary conditions
 constexpr int SP_OP_STENCIL_PER = 2;
 
+// whether a k_batch variant (FP32 or not, K load cases, kernel operator)
+// reads its stencil blocks from the pattern table, which it keeps in
+// SP_PT_BYTES of dynamic shared memory
+__host__ __device__ constexpr bool sp_batch_uses_ptable(bool fp32, int K, int op) {
+  return op == SP_OP_STENCIL && fp32 && K <= 6;
+}
+
 struct BatchPlan {
   MeshGeo geo; // node/element counts; h and vol per RVE
   const int *cols;
@@ -57,12 +64,15 @@ template <typename T, int K, int NT, int MINB, int CL, int OP>
 __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   constexpr bool PER = OP == SP_OP_STENCIL_PER;
   constexpr bool STENCIL = OP == SP_OP_STENCIL || PER;
+  // FP32 stencil under Dirichlet conditions: pattern table in dynamic shared memory
+  constexpr bool PT = sp_batch_uses_ptable(sizeof(T) == 4, K, OP);
   __shared__ double sKe[2 * SP_KE];
   // FP64 stencil tables for the residual (an FP64 stencil batch has them in sKeT already)
   constexpr bool OWN_KBD = !PER && !(STENCIL && sizeof(T) == 8);
   __shared__ __align__(16) double sKBd[OWN_KBD ? SP_KB_SIZE : 2];
   // element scatter values (assembled operator) or element blocks (stencil)
-  __shared__ __align__(16) T sKeT[STENCIL ? SP_KB_SIZE : 2 * SP_KE];
+  __shared__ __align__(16) T sKeT[STENCIL ? (PT ? 4 : SP_KB_SIZE) : 2 * SP_KE];
+  extern __shared__ __align__(16) float s_ptab[];  // SP_PT_BYTES when PT
   __shared__ double sD[72], sBbar[144], sdsh[192];
   // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
   __shared__ double red[33 * 16];
@@ -119,7 +129,10 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     if constexpr (STENCIL) {
       // 2s. no assembly: the stencil block tables and the Jacobi diagonal
       dinv = reinterpret_cast<T *>(P.ws_dinv) + (size_t)slot * P.drm_stride;
-      stencil_blocks<T>(t, NT, sKe, sKeT);
+      if constexpr (PT)
+        stencil_ptable(t, NT, sKe, s_ptab);
+      else
+        stencil_blocks<T>(t, NT, sKe, sKeT);
       if constexpr (PER)
         stencil_dinv_per<T>(gt, GNT, g, etype, sKe, dinv);
       else
@@ -166,7 +179,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     sa.eps = seps;
     sp_solve_info in;
     if constexpr (STENCIL) {
-      StencilOp<T, K, PER> op{sKeT, etype};
+      StencilOp<T, K, PER, PT> op{PT ? reinterpret_cast<const T *>(s_ptab) : sKeT, etype};
       in = solve_rve<T, K, NT, CL>(g, op, dinv, etype, sKe, sD, sBbar, u, r, x, p, q, sa, red,
                                    &sh, savg);
     } else {

@@ -694,6 +694,53 @@ __device__ inline void stencil_blocks(int t, int nt, const double *Ke /*[2][576]
   }
 }
 
+// Pattern tables of the FP32 stencil operator.  The block that couples a
+// node with its neighbour m = (dx+1) + 3(dy+1) + 9(dz+1) is the sum of the
+// element blocks of the sp_pt_n(m) elements the two nodes share (8 for the
+// node itself, 4 across a face, 2 across an edge, 1 across a corner); with
+// two materials it takes one of 2^sp_pt_n(m) values, one per material
+// pattern of those elements.  The table holds every one of them, summed in
+// FP64 and rounded once (416 blocks), so a node of any material mix reads
+// its 27 blocks directly instead of summing up to 64 element blocks.
+// Pattern bit i is the material of the i-th shared element in increasing
+// corner order c = ox + 2oy + 4oz (the element at (i-1+ox, j-1+oy, k-1+oz)).
+__host__ __device__ constexpr int sp_pt_n(int m) {
+  return (m % 3 == 1 ? 2 : 1) * ((m / 3) % 3 == 1 ? 2 : 1) * (m / 9 == 1 ? 2 : 1);
+}
+__host__ __device__ constexpr int sp_pt_off(int m) {
+  int o = 0;
+  for (int i = 0; i < m; i++) o += 1 << sp_pt_n(i);
+  return o;
+}
+constexpr int SP_PT_NREC = sp_pt_off(27);  // 416 blocks
+constexpr int SP_PT_REC = 12;              // floats per block (9 + 3 pads: 16-byte rows)
+constexpr int SP_PT_BYTES = SP_PT_NREC * SP_PT_REC * 4;
+static_assert(SP_PT_NREC == 256 + 6 * 16 + 12 * 4 + 8 * 2, "pattern table size");
+
+__device__ inline void stencil_ptable(int t, int nt, const double *Ke /*[2][576]*/, float *PT) {
+  for (int x = t; x < SP_PT_NREC * SP_PT_REC; x += nt) {
+    const int rec = x / SP_PT_REC, w = x % SP_PT_REC;
+    int m = 0;
+    while (m < 26 && sp_pt_off(m + 1) <= rec) m++;
+    const int p = rec - sp_pt_off(m);
+    const int dx = m % 3 - 1, dy = (m / 3) % 3 - 1, dz = m / 9 - 1;
+    double v = 0.0;
+    if (w < 9) {
+      const int d = w / 3, cc = w % 3;
+      int i = 0;
+      for (int c = 0; c < 8; c++) {
+        const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+        const int bx = 1 - ox + dx, by = 1 - oy + dy, bz = 1 - oz + dz;
+        if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+        const int la = hex8_local(1 - ox, 1 - oy, 1 - oz), lb = hex8_local(bx, by, bz);
+        v += Ke[((p >> i) & 1) * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
+        i++;
+      }
+    }
+    PT[x] = (float)v;
+  }
+}
+
 // Jacobi diagonal inverse of the stencil operator, component-major: for an
 // interior node 1 / sum over its 8 elements of Ke[type][3la+d][3la+d]
 // (summed in FP64, rounded once); 0 on boundary and padding nodes.
@@ -939,7 +986,10 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 // CG vectors vanish on the Dirichlet boundary) -- exactly the case in which
 // the adjacent lane holds a node of another row.  9 instead of 27 gathers
 // per value; the blocks, materials and output are those of spmm_stencil.
-template <int K>
+// PT: KB is the pattern table (stencil_ptable) and every lane reads its 27
+// blocks from it by the material pattern of the shared elements; otherwise
+// KB holds the stencil_blocks tables.
+template <int K, bool PT>
 __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const float *KB,
                                        const uint8_t *__restrict__ etype, const float *x,
                                        float *y, double *dot, unsigned amask, bool rev) {
@@ -972,8 +1022,8 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
       mask |= te << c;
       tb[c] = SP_KE_OFF + (int)te * SP_KB_TYPE;
     }
-    const bool all0 = __all_sync(FULL, !out || mask == 0u);
-    const bool all1 = __all_sync(FULL, !out || mask == 0xffu);
+    const bool all0 = PT || __all_sync(FULL, !out || mask == 0u);
+    const bool all1 = !PT && __all_sync(FULL, !out || mask == 0xffu);
     const bool pure = all0 || all1;
     const float *ka = KB + SP_KA_OFF + (all1 ? 27 * SP_KB_BLK : 0);
     float2 acc[3][KP];
@@ -1000,7 +1050,25 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
 #pragma unroll
         for (int dx = -1; dx <= 1; dx++) {
           float bv[9] = {};
-          if (pure) {
+          if constexpr (PT) {
+            // pattern bits of the shared elements: layer oz = 0 (q0) and oz = 1 (q1)
+            // of the (ox, oy) corners that the x and y offsets allow
+            unsigned q0 = 0, q1 = 0;
+            int nb = 0;
+#pragma unroll
+            for (int c2 = 0; c2 < 4; c2++) {
+              const int ox = c2 & 1, oy = c2 >> 1;
+              if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
+              q0 |= ((mask >> c2) & 1u) << nb;
+              q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
+              nb++;
+            }
+            const int m0 = (dx + 1) + 3 * (dy + 1);
+            const int idx = dz < 0 ? sp_pt_off(m0) + (int)q0
+                                   : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb))
+                                              : sp_pt_off(m0 + 18) + (int)q1);
+            add_block<float, float>(KB + idx * SP_PT_REC, bv);
+          } else if (pure) {
             add_block<float, float>(ka + ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) * SP_KB_BLK, bv);
           } else {
 #pragma unroll

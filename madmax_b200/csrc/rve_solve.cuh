@@ -130,15 +130,15 @@ struct EllOp {
   }
 };
 
-template <typename T, int K, bool PER = false>
+template <typename T, int K, bool PER = false, bool PT = false>
 struct StencilOp {
   static constexpr bool kBlocked = true;  // p node-blocked (nbk_base)
-  const T *kb;  // shared-memory element blocks (stencil_blocks)
+  const T *kb;  // shared-memory blocks: stencil_blocks, or stencil_ptable when PT
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
                         unsigned amask, bool rev) const {
     if constexpr (sizeof(T) == 4 && !PER && K <= 6)
-      spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+      spmm_stencil_xw<K, PT>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
     else
       spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
   }

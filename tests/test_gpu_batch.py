@@ -226,10 +226,12 @@ def test_large_rve_size_independent_properties():
     """A 40^3 RVE (206,763 dof), too large for the CPU oracle in a test:
     the stencil and assembled operators agree, the tangent is symmetric
     (major symmetry of the homogenized stiffness), its diagonal is positive,
-    and the periodic tangent is bounded by it (Hill)."""
+    and the periodic tangent is bounded by it (Hill).  The two operators are
+    compared at a 1e-10 residual: at 1e-8 the tangents of two different FP32
+    iterations of this large RVE can differ by ~1e-7 of their scale."""
     d = make_descs(40, [40])[0]
-    a, _, ia = mb.Batch([d]).homogenize()
-    b, _, ib = mb.Batch([d], op=mb.SP_OP_ELL).homogenize()
+    a, _, ia = mb.Batch([d], rtol=1e-10).homogenize()
+    b, _, ib = mb.Batch([d], op=mb.SP_OP_ELL, rtol=1e-10).homogenize()
     p, _, ip = mb.Batch([d], bc=mb.SP_BC_PERIODIC).homogenize()
     for inf in (ia, ib, ip):
         assert (mb.info_array(inf)["status"] == 0).all()
