@@ -247,13 +247,15 @@ def test_large_rve_size_independent_properties():
 def test_larger_sizes_stencil_agrees_with_assembled():
     """The bench's larger sizes and beyond (n = 16 ... 28) on the stencil at
     both one-CTA-per-SM shapes give the assembled operator's tangent, which
-    is tested against the oracle."""
+    is tested against the oracle.  Compared at a 1e-10 residual, so that the
+    two operators' different FP32 iterations cannot separate the tangents by
+    more than the tolerance."""
     descs = make_descs(77, [16, 20, 24, 28, 20])
     for threads in (1024, 512):
-        a, _, ia = mb.Batch(descs, threads=threads, ctas_per_sm=1).homogenize()
+        a, _, ia = mb.Batch(descs, threads=threads, ctas_per_sm=1, rtol=1e-10).homogenize()
         assert (mb.info_array(ia)["status"] == 0).all()
         if threads == 1024:
-            b, _, ib = mb.Batch(descs, op=mb.SP_OP_ELL).homogenize()
+            b, _, ib = mb.Batch(descs, op=mb.SP_OP_ELL, rtol=1e-10).homogenize()
             assert (mb.info_array(ib)["status"] == 0).all()
         for i in range(len(descs)):
             assert np.abs(a[i] - b[i]).max() <= 2e-8 * np.abs(b[i]).max(), (threads, i)
