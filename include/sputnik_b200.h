@@ -194,9 +194,10 @@ typedef struct {
   double inner_rtol; /* CG residual reduction per refinement step (default 1e-4) */
   int max_outer;     /* refinement steps (default 8) */
   int max_inner;     /* CG iterations per step (default 4000) */
-  int threads;       /* threads per CTA (0: 1024 for the stencil, 512 otherwise) */
+  int threads;       /* threads per CTA (0: 512) */
   int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
-  int ctas_per_sm;   /* resident CTAs per SM: 1 (1024 threads), 1 or 2 (512), 2 or 4 (256); 0: 1 or 2 */
+  int ctas_per_sm;   /* resident CTAs per SM: 1 (1024 threads), 1 or 2 (512), 2 or 4 (256);
+                        0: 1 for the FP32 stencil under affine conditions, else 2 */
   int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 (assembled) */
   int op;            /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int bc;            /* SP_BC_AFFINE (default) or SP_BC_PERIODIC (stencil only) */
