@@ -985,11 +985,10 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 // lanes (shuffles), or are 0 where that neighbour is a boundary node (the
 // CG vectors vanish on the Dirichlet boundary) -- exactly the case in which
 // the adjacent lane holds a node of another row.  9 instead of 27 gathers
-// per value; the blocks, materials and output are those of spmm_stencil.
-// PT: KB is the pattern table (stencil_ptable) and every lane reads its 27
-// blocks from it by the material pattern of the shared elements; otherwise
-// KB holds the stencil_blocks tables.
-template <int K, bool PT>
+// per value; the materials and output are those of spmm_stencil.  KB is
+// the pattern table (stencil_ptable): every lane reads its 27 blocks from
+// it by the material pattern of the elements it shares with each neighbour.
+template <int K>
 __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const float *KB,
                                        const uint8_t *__restrict__ etype, const float *x,
                                        float *y, double *dot, unsigned amask, bool rev) {
@@ -1012,20 +1011,13 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
     const int a = i + j * sy + k * sz;
     // the adjacent lanes hold the x-neighbours unless those are boundary nodes
     const bool lo = ii > 0, hi = ii < mx - 1;
-    int tb[8];  // offset of the element's material blocks in KB
-    unsigned mask = 0;
+    unsigned mask = 0;  // bit c: material of the element at corner c
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
       const int e = (i - 1 + ox) + (j - 1 + oy) * esy + (k - 1 + oz) * esz;
-      const unsigned te = __ldg(etype + e);
-      mask |= te << c;
-      tb[c] = SP_KE_OFF + (int)te * SP_KB_TYPE;
+      mask |= (unsigned)__ldg(etype + e) << c;
     }
-    const bool all0 = PT || __all_sync(FULL, !out || mask == 0u);
-    const bool all1 = !PT && __all_sync(FULL, !out || mask == 0xffu);
-    const bool pure = all0 || all1;
-    const float *ka = KB + SP_KA_OFF + (all1 ? 27 * SP_KB_BLK : 0);
     float2 acc[3][KP];
 #pragma unroll
     for (int d = 0; d < 3; d++)
@@ -1049,40 +1041,24 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
           }
 #pragma unroll
         for (int dx = -1; dx <= 1; dx++) {
-          float bv[9] = {};
-          if constexpr (PT) {
-            // pattern bits of the shared elements: layer oz = 0 (q0) and oz = 1 (q1)
-            // of the (ox, oy) corners that the x and y offsets allow
-            unsigned q0 = 0, q1 = 0;
-            int nb = 0;
+          // pattern bits of the shared elements: layer oz = 0 (q0) and oz = 1
+          // (q1) of the (ox, oy) corners that the x and y offsets allow
+          unsigned q0 = 0, q1 = 0;
+          int nb = 0;
 #pragma unroll
-            for (int c2 = 0; c2 < 4; c2++) {
-              const int ox = c2 & 1, oy = c2 >> 1;
-              if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
-              q0 |= ((mask >> c2) & 1u) << nb;
-              q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
-              nb++;
-            }
-            const int m0 = (dx + 1) + 3 * (dy + 1);
-            const int idx = dz < 0 ? sp_pt_off(m0) + (int)q0
-                                   : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb))
-                                              : sp_pt_off(m0 + 18) + (int)q1);
-            add_block<float, float>(KB + idx * SP_PT_REC, bv);
-          } else if (pure) {
-            add_block<float, float>(ka + ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) * SP_KB_BLK, bv);
-          } else {
-#pragma unroll
-            for (int c = 0; c < 8; c++) {
-              const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
-              const int bx = 1 - ox + dx, by = 1 - oy + dy;
-              if (bx < 0 || bx > 1 || by < 0 || by > 1) continue;  // resolved at compile time
-              const int bz = 1 - oz + dz;                            // warp-uniform
-              if (bz < 0 || bz > 1) continue;
-              const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
-              const int lb = hex8_local(bx, by, 0) + 4 * bz;
-              add_block<float, float>(KB + tb[c] + (la * 8 + lb) * SP_KB_BLK, bv);
-            }
+          for (int c2 = 0; c2 < 4; c2++) {
+            const int ox = c2 & 1, oy = c2 >> 1;
+            if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
+            q0 |= ((mask >> c2) & 1u) << nb;
+            q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
+            nb++;
           }
+          const int m0 = (dx + 1) + 3 * (dy + 1);
+          const int idx = dz < 0 ? sp_pt_off(m0) + (int)q0
+                                 : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb))
+                                            : sp_pt_off(m0 + 18) + (int)q1);
+          float bv[9] = {};
+          add_block<float, float>(KB + idx * SP_PT_REC, bv);
 #pragma unroll
           for (int p = 0; p < KP; p++) {
             if (!((amask >> (2 * p)) & 3u)) continue;

@@ -132,13 +132,15 @@ struct EllOp {
 
 template <typename T, int K, bool PER = false, bool PT = false>
 struct StencilOp {
+  static_assert(!PT || (sizeof(T) == 4 && !PER && K <= 6),
+                "pattern tables serve the FP32 Dirichlet stencil with at most 6 load cases");
   static constexpr bool kBlocked = true;  // p node-blocked (nbk_base)
   const T *kb;  // shared-memory blocks: stencil_blocks, or stencil_ptable when PT
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
                         unsigned amask, bool rev) const {
-    if constexpr (sizeof(T) == 4 && !PER && K <= 6)
-      spmm_stencil_xw<K, PT>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+    if constexpr (PT)
+      spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
     else
       spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
   }
