@@ -66,6 +66,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   constexpr bool STENCIL = OP == SP_OP_STENCIL || PER;
   // FP32 stencil under Dirichlet conditions: pattern table in dynamic shared memory
   constexpr bool PT = sp_batch_uses_ptable(sizeof(T) == 4, K, OP);
+  constexpr bool WIDE = NT * MINB <= 512;  // 128 registers a thread
   __shared__ double sKe[2 * SP_KE];
   // FP64 stencil tables for the residual (an FP64 stencil batch has them in sKeT already)
   constexpr bool OWN_KBD = !PER && !(STENCIL && sizeof(T) == 8);
@@ -180,12 +181,12 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     sp_solve_info in;
     if constexpr (STENCIL) {
       StencilOp<T, K, PER, PT> op{PT ? reinterpret_cast<const T *>(s_ptab) : sKeT, etype};
-      in = solve_rve<T, K, NT, CL>(g, op, dinv, etype, sKe, sD, sBbar, u, r, x, p, q, sa, red,
-                                   &sh, savg);
+      in = solve_rve<T, K, NT, CL, decltype(op), WIDE>(g, op, dinv, etype, sKe, sD, sBbar, u, r,
+                                                       x, p, q, sa, red, &sh, savg);
     } else {
       EllOp<T, K> op{nsv, pl.nbr};
-      in = solve_rve<T, K, NT, CL>(g, op, dinv, etype, sKe, sD, sBbar, u, r, x, p, q, sa, red,
-                                   &sh, savg);
+      in = solve_rve<T, K, NT, CL, decltype(op), WIDE>(g, op, dinv, etype, sKe, sD, sBbar, u, r,
+                                                       x, p, q, sa, red, &sh, savg);
     }
     if (t == 0 && rank == 0) {
       for (int qq = 0; qq < P.nrhs; qq++) {

@@ -169,7 +169,9 @@ struct V16 {
 // <strain>_q, avg[q*12 + 6..11] = <stress>_q (q < nrhs, shared memory of
 // every CTA) and the return value describes the solve.  red: shared scratch
 // of 33*16 doubles; sh: shared CG scalars.
-template <typename T, int K, int NT, int CL, typename Op>
+// WIDE: the kernel has 128 registers a thread (at most 512 threads per SM),
+// room for the per-node FP64 residual.
+template <typename T, int K, int NT, int CL, typename Op, bool WIDE = false>
 __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv,
                                    const uint8_t *etype, const double *sKe, const double *sD,
                                    const double *sBbar, double *u, T *r, T *x, T *p, T *q,
@@ -288,7 +290,10 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         if (first)
           residual_stencil<K, T, true>(gt, GNT, g, etype, P.kbd, u, r, m1, m1 + K);
         else
-          residual_stencil<K, T>(gt, GNT, g, etype, P.kbd, u, r, m1);
+          if constexpr (WIDE)
+            residual_stencil_node<K, T>(gt, GNT, g, etype, P.kbd, u, r, m1);
+          else
+            residual_stencil<K, T>(gt, GNT, g, etype, P.kbd, u, r, m1);
       } else {
         if (first)
           residual_soa<K, T, false, true>(gt, GNT, g, etype, sKe, u, r, m1, m1 + K);
