@@ -132,8 +132,7 @@ struct EllOp {
 
 template <typename T, int K, bool PER = false, bool PT = false>
 struct StencilOp {
-  static_assert(!PT || (sizeof(T) == 4 && !PER && K <= 6),
-                "pattern tables serve the FP32 Dirichlet stencil with at most 6 load cases");
+  static_assert(!PT || (sizeof(T) == 4 && !PER), "pattern tables serve the FP32 Dirichlet stencil");
   static constexpr bool kBlocked = true;  // p node-blocked (nbk_base)
   const T *kb;  // shared-memory blocks: stencil_blocks, or stencil_ptable when PT
   const uint8_t *etype;

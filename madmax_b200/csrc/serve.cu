@@ -202,8 +202,12 @@ __global__ void __launch_bounds__(SERVE_NT) k_serve_gram(ServeGeom *geoms, int n
 template <int OP, int MINB>
 __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
   constexpr bool STENCIL = OP == SP_OP_STENCIL;
+  // one request slot per SM (128 registers a thread): the stencil reads its
+  // blocks from the pattern table, in SP_PT_BYTES of dynamic shared memory
+  constexpr bool PT = STENCIL && MINB == 1;
   __shared__ double sKe[2 * SP_KE], sD[72], sB[144];
-  __shared__ __align__(16) float sKB[STENCIL ? SP_KB_SIZE : 4];
+  __shared__ __align__(16) float sKB[STENCIL && !PT ? SP_KB_SIZE : 4];
+  extern __shared__ __align__(16) float s_ptab[];
   __shared__ __align__(16) double sKBd[SP_KB_SIZE];  // FP64 stencil tables (residual)
   __shared__ double red[33 * 16];
   __shared__ double savg[SP_MAX_RHS * 12];
@@ -352,7 +356,10 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
       }
     }
     __syncthreads();
-    if constexpr (STENCIL) stencil_blocks<float>(t, SERVE_NT, sKe, sKB);
+    if constexpr (PT)
+      stencil_ptable(t, SERVE_NT, sKe, s_ptab);
+    else if constexpr (STENCIL)
+      stencil_blocks<float>(t, SERVE_NT, sKe, sKB);
     stencil_blocks<double>(t, SERVE_NT, sKe, sKBd);
     affine_soa<SERVE_K>(t, SERVE_NT, g, seps, SERVE_NRHS, warm, u);
     __syncthreads();
@@ -371,13 +378,14 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     sa.eps = nullptr;  // affine conditions: eps is carried by u's boundary values
     sp_solve_info in;
     if constexpr (STENCIL) {
-      StencilOp<float, SERVE_K> op{sKB, G.etype};
-      in = solve_rve<float, SERVE_K, SERVE_NT, 1>(g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p,
-                                                  q, sa, red, &sh, savg);
+      // one request slot per SM has 128 registers a thread: per-node FP64 residual
+      StencilOp<float, SERVE_K, false, PT> op{PT ? s_ptab : sKB, G.etype};
+      in = solve_rve<float, SERVE_K, SERVE_NT, 1, decltype(op), MINB == 1>(
+          g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p, q, sa, red, &sh, savg);
     } else {
       EllOp<float, SERVE_K> op{G.vals, G.nbr};
-      in = solve_rve<float, SERVE_K, SERVE_NT, 1>(g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p,
-                                                  q, sa, red, &sh, savg);
+      in = solve_rve<float, SERVE_K, SERVE_NT, 1, decltype(op), MINB == 1>(
+          g, op, G.dinv, G.etype, sKe, sD, sB, u, r, x, p, q, sa, red, &sh, savg);
     }
     // keep this request's solutions and strains as the geometry's next warm
     // start when it ran a refinement step (they then meet refine_rtol); a
@@ -452,6 +460,11 @@ using ServeFn = void (*)(ServeParams);
 static ServeFn serve_kernel(const sp_server_opts &o) {
   if (o.op == SP_OP_ELL) return o.ctas_per_sm == 1 ? k_serve<SP_OP_ELL, 1> : k_serve<SP_OP_ELL, 2>;
   return o.ctas_per_sm == 1 ? k_serve<SP_OP_STENCIL, 1> : k_serve<SP_OP_STENCIL, 2>;
+}
+
+// its dynamic shared memory: the pattern table of the one-slot stencil loop
+static int serve_dyn_smem(const sp_server_opts &o) {
+  return (o.op == SP_OP_STENCIL && o.ctas_per_sm == 1) ? SP_PT_BYTES : 0;
 }
 
 extern "C" void sp_server_opts_default(sp_server_opts *o) {
@@ -700,7 +713,11 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
 // dispatcher's counter): the grid never exceeds what the SMs hold.
 static int server_grid(sp_server *s, Device *d) {
   int occ = 0;
-  SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, serve_kernel(s->o), SERVE_NT, 0));
+  const int dyn = serve_dyn_smem(s->o);
+  if (dyn)
+    SP_CUDA_TRY(cudaFuncSetAttribute((const void *)serve_kernel(s->o),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+  SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, serve_kernel(s->o), SERVE_NT, dyn));
   if (occ < 1) return sp_set_error(SP_ERR_CUDA, "serving kernel does not fit an SM");
   int cap = d->nsm * occ;
   if (s->grid > cap) s->grid = cap;
@@ -715,7 +732,7 @@ static int server_launch(sp_server *s) {
   z.dispatcher_gone = 0;
   SP_CUDA_TRY(cudaMemcpyAsync(s->d_dev, &z, sizeof(z), cudaMemcpyHostToDevice, s->stream));
   SP_CUDA_TRY(cudaStreamSynchronize(s->stream));
-  serve_kernel(s->o)<<<s->grid, SERVE_NT, 0, s->stream>>>(s->P);
+  serve_kernel(s->o)<<<s->grid, SERVE_NT, serve_dyn_smem(s->o), s->stream>>>(s->P);
   SP_CUDA_TRY(cudaGetLastError());
   s->running = 1;
   return SP_OK;
