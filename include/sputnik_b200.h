@@ -211,6 +211,12 @@ typedef struct sp_batch_s sp_batch;
  * values and the per-CTA work space on the GPU. */
 int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batch_opts *o, sp_batch **out);
 int sp_batch_destroy(sp_batch *b);
+/* Replaces the element materials of RVE `rve` (nelm bytes on the host, 0 =
+ * matrix, 1 = fibre, elements x-fastest) for the following launches, in
+ * place of its fibre-cylinder classification: any two-material voxel
+ * micro-structure.  No counterpart in the reference, whose micro-structures
+ * are the fibre cylinders of micro/src/micro_struct.c. */
+int sp_batch_set_etype(sp_batch *b, int rve, const unsigned char *etype, void *stream);
 /* Bytes of device memory held by the batch. */
 int sp_batch_device_bytes(const sp_batch *b, size_t *bytes);
 /* Queue the host->device copy of the step's inputs on `stream`:

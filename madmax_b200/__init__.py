@@ -179,6 +179,7 @@ _PROTOS = {
     "sp_batch_create": (C.c_int, [C.c_int, C.POINTER(sp_rve_desc), C.POINTER(sp_batch_opts),
                                   C.POINTER(_vp)]),
     "sp_batch_destroy": (C.c_int, [_vp]),
+    "sp_batch_set_etype": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_ubyte), _vp]),
     "sp_batch_device_bytes": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "sp_batch_shape": (C.c_int, [_vp, _ip, _ip, _ip]),
     "sp_batch_upload": (C.c_int, [_vp, _dp, _dp, _vp]),
@@ -428,6 +429,13 @@ class Batch:
     def upload(self, strains=None, materials=None, stream=None):
         check(lib().sp_batch_upload(self.h, ptr(strains), ptr(materials), stream),
               "sp_batch_upload")
+
+    def set_etype(self, rve: int, etype, stream=None):
+        """Element materials of RVE `rve` (0 matrix, 1 fibre, x-fastest) in
+        place of its fibre classification, from the next launch on."""
+        et = np.ascontiguousarray(etype, dtype=np.uint8)
+        check(lib().sp_batch_set_etype(self.h, int(rve), et.ctypes.data_as(C.POINTER(C.c_ubyte)),
+                                       stream), "sp_batch_set_etype")
 
     def launch(self, stream=None):
         check(lib().sp_batch_launch(self.h, stream), "sp_batch_launch")

@@ -78,6 +78,8 @@ using namespace sp;
 struct sp_batch_s {
   int nrve = 0, nrhs = 6, kp = 6, dev = -1, grid = 0, last_launches = 0;
   int dyn_smem = 0;  // dynamic shared memory of the kernel (pattern table)
+  std::vector<long long> etype_off;  // per RVE: its materials in d_etype
+  std::vector<int> nelm;
   sp_batch_opts o;
   std::vector<DevPlan *> plans;
   std::vector<sp_rve_desc> descs;
@@ -222,6 +224,8 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     }
     maxdof = std::max(maxdof, g.ndof);
     maxnp = std::max(maxnp, g.nn_pad);
+    b->etype_off.push_back(r.etype_off);
+    b->nelm.push_back(g.nelm);
   }
   // host-side classification into one pinned staging buffer
   uint8_t *et = nullptr;
@@ -385,6 +389,24 @@ extern "C" int sp_batch_upload(sp_batch *b, const double *strains, const double 
   if (materials)
     SP_CUDA_TRY(cudaMemcpyAsync(b->d_mats, materials, (size_t)b->nrve * 4 * sizeof(double),
                                 cudaMemcpyHostToDevice, s));
+  return SP_OK;
+}
+
+extern "C" int sp_batch_set_etype(sp_batch *b, int rve, const unsigned char *etype, void *stream) {
+  if (!b || !etype) return sp_set_error(SP_ERR_ARG, "sp_batch_set_etype: null argument");
+  if (rve < 0 || rve >= b->nrve)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_set_etype: RVE %d of %d", rve, b->nrve);
+  for (int e = 0; e < b->nelm[rve]; e++)
+    if (etype[e] > 1)
+      return sp_set_error(SP_ERR_ARG, "sp_batch_set_etype: element %d has material %d (0 or 1)", e,
+                          (int)etype[e]);
+  Device *d;
+  SP_TRY(device(&d));
+  cudaStream_t s = pick_stream(stream, d);
+  SP_CUDA_TRY(cudaMemcpyAsync(b->d_etype + b->etype_off[rve], etype, (size_t)b->nelm[rve],
+                              cudaMemcpyHostToDevice, s));
+  // a pageable source is read before the call returns; the copy is ordered
+  // before the stream's next launch
   return SP_OK;
 }
 
