@@ -266,10 +266,14 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
   float *ws = P.ws_v + (size_t)blockIdx.x * 4 * P.stride;
   float *r = ws, *x = ws + P.stride, *p = ws + 2 * P.stride, *q = ws + 3 * P.stride;
   for (;;) {
-    // claim the next published request (bounded wait)
+    // claim the next published request (bounded wait).  The dispatcher's
+    // idle limit decides when the loop returns: a slot leaves when the
+    // dispatcher has left or stop is set.  Its own bound, 8 times the
+    // dispatcher's, is a safeguard only: slots that left one by one on their
+    // own idle count would starve a loop whose dispatcher still runs.
     if (t == 0) {
       long long job = -1;
-      int idle = 0;
+      long long idle = 0;
       for (;;) {
         unsigned long long h = *(volatile unsigned long long *)&D->claim;
         long long dt = D->dtail;
@@ -280,7 +284,7 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
           }
           continue;
         }
-        if (D->dstop || D->dispatcher_gone || ++idle > P.idle_limit) break;
+        if (D->dstop || D->dispatcher_gone || ++idle > 8LL * P.idle_limit) break;
         __nanosleep(500);
       }
       __threadfence();
@@ -436,6 +440,7 @@ using namespace sp;
 
 struct sp_server_s {
   int ngeom = 0, dev = -1, grid = 0, cap = 0, running = 0;
+  double last_alive = 0.0;  // host time of the last liveness check of the loop
   sp_server_opts o;
   std::vector<DevPlan *> plans;
   std::vector<ServeGeom> hgeoms;
@@ -739,8 +744,16 @@ static int server_launch(sp_server *s) {
 }
 
 // relaunch the loop if it went idle while requests are pending
+// The loop's liveness check (a stream query, microseconds of driver time)
+// runs at most every SP_KEEPALIVE_S: submit and poll call it once per
+// request, thousands of times a millisecond under load.
+constexpr double SP_KEEPALIVE_S = 50e-6;
+
 static int server_keepalive(sp_server *s) {
   if (!s->running) return SP_OK;
+  const double t = now_s();
+  if (t - s->last_alive < SP_KEEPALIVE_S) return SP_OK;
+  s->last_alive = t;
   cudaError_t q = cudaStreamQuery(s->stream);
   if (q == cudaErrorNotReady) return SP_OK;
   if (q != cudaSuccess) return sp_set_error(SP_ERR_CUDA, "serving loop failed: %s", cudaGetErrorString(q));
