@@ -86,6 +86,19 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   const int gt = rank * NT + t;
   constexpr int GNT = CL * NT;
   const int slot = blockIdx.x / CL;  // work space of this cluster
+  if constexpr (PT) {
+    // launched without the pattern table's shared memory: solve nothing,
+    // mark every RVE this CTA would have taken as failed
+    if (dynamic_smem_bytes() < (unsigned)SP_PT_BYTES) {
+      if (t == 0 && rank == 0)
+        for (int job = slot; job < P.nrve; job += gridDim.x / CL) {
+          sp_solve_info bad = {};
+          bad.status = SP_ERR_STATE;
+          P.out_info[P.order[job]] = bad;
+        }
+      return;
+    }
+  }
   double *u = P.ws_u + (size_t)slot * P.ws_stride;
   T *ws = reinterpret_cast<T *>(P.ws_v) + (size_t)slot * 4 * P.ws_stride;
   T *r = ws, *x = ws + P.ws_stride, *p = ws + 2 * P.ws_stride, *q = ws + 3 * P.ws_stride;

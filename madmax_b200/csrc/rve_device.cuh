@@ -717,6 +717,15 @@ constexpr int SP_PT_REC = 12;              // floats per block (9 + 3 pads: 16-b
 constexpr int SP_PT_BYTES = SP_PT_NREC * SP_PT_REC * 4;
 static_assert(SP_PT_NREC == 256 + 6 * 16 + 12 * 4 + 8 * 2, "pattern table size");
 
+// Bytes of dynamic shared memory the running kernel was launched with.  A
+// kernel that keeps the pattern table there checks it first: a launch
+// without it would read and write past the block's shared memory.
+__device__ inline unsigned dynamic_smem_bytes() {
+  unsigned v;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
+  return v;
+}
+
 __device__ inline void stencil_ptable(int t, int nt, const double *Ke /*[2][576]*/, float *PT) {
   for (int x = t; x < SP_PT_NREC * SP_PT_REC; x += nt) {
     const int rec = x / SP_PT_REC, w = x % SP_PT_REC;

@@ -262,6 +262,9 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     return;
   }
 
+  // a slot launched without the pattern table's shared memory serves nothing
+  // (the host's waits are bounded)
+  if (PT && dynamic_smem_bytes() < (unsigned)SP_PT_BYTES) return;
   double *u = P.ws_u + (size_t)blockIdx.x * P.stride;
   float *ws = P.ws_v + (size_t)blockIdx.x * 4 * P.stride;
   float *r = ws, *x = ws + P.stride, *p = ws + 2 * P.stride, *q = ws + 3 * P.stride;
