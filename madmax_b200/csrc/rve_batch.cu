@@ -248,7 +248,10 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
                         "cluster %d, %s operator in this precision", o.threads, o.ctas_per_sm,
                         o.cluster, o.op == SP_OP_ELL ? "assembled" : "stencil");
     int g = d->nsm * o.ctas_per_sm;
-    b->dyn_smem = sp_batch_uses_ptable(o.precision == SP_PREC_MIXED, kp, kernel_op(o)) ? SP_PT_BYTES : 0;
+    b->dyn_smem = sp_batch_uses_ptable(o.precision == SP_PREC_MIXED, kp, kernel_op(o),
+                                       o.threads * o.ctas_per_sm <= 512)
+                      ? SP_PT_BYTES
+                      : 0;
     if (fn && !rc && b->dyn_smem) {
       if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                b->dyn_smem) != cudaSuccess) {

@@ -12,11 +12,12 @@ namespace sp {
 // periodic boundary conditions
 constexpr int SP_OP_STENCIL_PER = 2;
 
-// whether a k_batch variant (FP32 or not, K load cases, kernel operator)
-// reads its stencil blocks from the pattern table, which it keeps in
-// SP_PT_BYTES of dynamic shared memory
-__host__ __device__ constexpr bool sp_batch_uses_ptable(bool fp32, int K, int op) {
-  return op == SP_OP_STENCIL && fp32 && K <= 6;
+// whether a k_batch variant (FP32 or not, K load cases, kernel operator,
+// 128 registers a thread) reads its stencil blocks from the pattern table,
+// which it keeps in SP_PT_BYTES of dynamic shared memory; more than 6 load
+// cases need the wide register budget
+__host__ __device__ constexpr bool sp_batch_uses_ptable(bool fp32, int K, int op, bool wide = false) {
+  return op == SP_OP_STENCIL && fp32 && (K <= 6 || wide);
 }
 
 struct BatchPlan {
@@ -65,8 +66,8 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   constexpr bool PER = OP == SP_OP_STENCIL_PER;
   constexpr bool STENCIL = OP == SP_OP_STENCIL || PER;
   // FP32 stencil under Dirichlet conditions: pattern table in dynamic shared memory
-  constexpr bool PT = sp_batch_uses_ptable(sizeof(T) == 4, K, OP);
   constexpr bool WIDE = NT * MINB <= 512;  // 128 registers a thread
+  constexpr bool PT = sp_batch_uses_ptable(sizeof(T) == 4, K, OP, WIDE);
   __shared__ double sKe[2 * SP_KE];
   // FP64 stencil tables for the residual (an FP64 stencil batch has them in sKeT already)
   constexpr bool OWN_KBD = !PER && !(STENCIL && sizeof(T) == 8);
