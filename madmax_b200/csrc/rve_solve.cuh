@@ -13,7 +13,10 @@
 // (deterministic, independent of scheduling).  Cluster barriers separate
 // the phases in which a CTA reads rows another CTA wrote (the SpMM gathers,
 // the residual gathers of u).  Vectors are component-major,
-// v[(k*3 + d)*nn_pad + node], padding nodes zero.
+// v[(k*3 + d)*nn_pad + node], padding nodes zero; the stencil operator's
+// input p is node-blocked (nbk_base).  The corrections are reliable updates
+// of one CG recurrence: each refinement step replaces r by the true FP64
+// residual and keeps the search direction.
 #pragma once
 
 #include <cooperative_groups.h>
