@@ -214,8 +214,10 @@ int sp_batch_destroy(sp_batch *b);
 /* Replaces the element materials of RVE `rve` (nelm bytes on the host, 0 =
  * matrix, 1 = fibre, elements x-fastest) for the following launches, in
  * place of its fibre-cylinder classification: any two-material voxel
- * micro-structure.  No counterpart in the reference, whose micro-structures
- * are the fibre cylinders of micro/src/micro_struct.c. */
+ * micro-structure.  The copy runs on `stream` before its next launch; keep a
+ * pinned `etype` unchanged until the stream has reached it.  No counterpart
+ * in the reference, whose micro-structures are the fibre cylinders of
+ * micro/src/micro_struct.c. */
 int sp_batch_set_etype(sp_batch *b, int rve, const unsigned char *etype, void *stream);
 /* Bytes of device memory held by the batch. */
 int sp_batch_device_bytes(const sp_batch *b, size_t *bytes);

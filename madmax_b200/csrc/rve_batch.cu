@@ -408,8 +408,8 @@ extern "C" int sp_batch_set_etype(sp_batch *b, int rve, const unsigned char *ety
   cudaStream_t s = pick_stream(stream, d);
   SP_CUDA_TRY(cudaMemcpyAsync(b->d_etype + b->etype_off[rve], etype, (size_t)b->nelm[rve],
                               cudaMemcpyHostToDevice, s));
-  // a pageable source is read before the call returns; the copy is ordered
-  // before the stream's next launch
+  // ordered before the stream's next launch; a pinned source is read
+  // asynchronously, so the caller keeps it until the stream reaches the copy
   return SP_OK;
 }
 
