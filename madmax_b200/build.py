@@ -23,8 +23,10 @@ BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libsputnik_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -static-global-template-stub=false: the batched kernel's instantiations live
+# in their own translation units and are launched from rve_batch.cu
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-              "-Xptxas", "-v"] + ARCH
+              "-static-global-template-stub=false", "-Xptxas", "-v"] + ARCH
 CC_FLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function"]
 
 

@@ -1,6 +1,7 @@
 /*
  * sp_internal.h -- declarations shared by the C and CUDA translation units
- * of libsputnik_b200.so.  Not installed; the public ABI is include/*.h.
+ * of libsputnik_b200.so.  Not installed; the public ABI is the headers in
+ * include/.
  */
 #ifndef SP_INTERNAL_H
 #define SP_INTERNAL_H
