@@ -254,7 +254,8 @@ typedef struct {
   int queue_capacity;   /* request ring size (0: 65536) */
   double rtol;          /* default 1e-8 */
   double inner_rtol;    /* CG residual reduction per refinement step (default 1e-4) */
-  int idle_spin_limit;  /* empty polls before the loop returns (0: default) */
+  int idle_spin_limit;  /* empty polls of the dispatcher before the loop returns (0: default
+                           2,000,000); the next submit relaunches it */
   int op;               /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int ctas_per_sm;      /* request slots per SM: 1 or 2 (0: 1 for the stencil, 2 for ELL) */
   double refine_rtol;   /* a request whose warm-start prediction misses rtol is solved to
