@@ -197,7 +197,7 @@ typedef struct {
   int threads;       /* threads per CTA (0: 512) */
   int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
   int ctas_per_sm;   /* resident CTAs per SM: 1 (1024 threads), 1 or 2 (512), 2 or 4 (256);
-                        0: 1 for the FP32 stencil under affine conditions, else 2 */
+                        0: 1 for the stencil, 2 for the assembled operator */
   int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 (assembled) */
   int op;            /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int bc;            /* SP_BC_AFFINE (default) or SP_BC_PERIODIC (stencil only) */

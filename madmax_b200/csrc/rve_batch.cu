@@ -136,12 +136,12 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (o.precision != SP_PREC_MIXED && o.precision != SP_PREC_FP64)
     return sp_set_error(SP_ERR_ARG, "sp_batch_create: unknown precision");
   // CTA shape: 512 threads x 1 or 2 CTAs per SM, 256 threads x 2 or 4, or
-  // (stencil operator) 1024 threads x 1.  Unset: 512 x 1 for the FP32
-  // stencil under affine conditions (128 registers a thread, no spills; as
-  // fast as 1024 x 1 on n = 16-20, 20-26% faster on n = 8-12), 512 x 2
-  // otherwise.
-  const bool one = o.op == SP_OP_STENCIL && o.bc == SP_BC_AFFINE && o.cluster <= 1 &&
-                   o.precision == SP_PREC_MIXED;
+  // (stencil operator) 1024 threads x 1.  Unset: 512 x 1 for the stencil
+  // (128 registers a thread: as fast as 1024 x 1 on affine n = 16-20 and
+  // 20-26% faster on n = 8-12; 2.3x faster than 512 x 2 under periodic
+  // conditions, whose 64-register build spills), 512 x 2 for the assembled
+  // operator.
+  const bool one = o.op == SP_OP_STENCIL && o.cluster <= 1;
   if (o.threads == 0) o.threads = 512;
   if (o.ctas_per_sm == 0) o.ctas_per_sm = (o.threads == 1024 || (one && o.threads == 512)) ? 1 : 2;
   if (o.threads != 256 && o.threads != 512 && o.threads != 1024)

@@ -193,8 +193,9 @@ def test_default_shape_per_operator():
     descs = make_descs(2, [4, 5])
     assert mb.Batch(descs).shape()[:2] == (512, 1)
     assert mb.Batch(descs, op=mb.SP_OP_ELL).shape()[:2] == (512, 2)
-    assert mb.Batch(descs, bc=mb.SP_BC_PERIODIC).shape()[:2] == (512, 2)
-    assert mb.Batch(descs, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 2)
+    assert mb.Batch(descs, bc=mb.SP_BC_PERIODIC).shape()[:2] == (512, 1)
+    assert mb.Batch(descs, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 1)
+    assert mb.Batch(descs, op=mb.SP_OP_ELL, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 2)
 
 
 # --------------------------------------------------- edge and full sizes ---
