@@ -218,3 +218,20 @@ def test_no_device_no_fallback():
     h = mb._vp()
     assert mb.lib().sp_rve_create(C.byref(mb.rve_desc(2)), C.byref(h)) == mb.SP_ERR_CUDA
     assert "CUDA" in mb.last_error() or "device" in mb.last_error()
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c11"), ("g++", "-std=c++17")])
+def test_public_headers_compile_standalone(tmp_path, compiler, std):
+    """Each public header is self-contained C (and C++): a translation unit
+    that includes only it compiles without warnings."""
+    import shutil
+    import subprocess
+    if not shutil.which(compiler):
+        pytest.skip(f"{compiler} not found")
+    for h in ("ell.h", "fem.h", "solvers.h", "sputnik_b200.h"):
+        src = tmp_path / ("inc.c" if compiler == "gcc" else "inc.cpp")
+        src.write_text(f'#include "{h}"\nint sp_header_probe(void) {{ return 0; }}\n')
+        r = subprocess.run([compiler, std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                            "-I", os.path.join(ROOT, "include"), str(src)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, (h, r.stderr[-2000:])
