@@ -4,8 +4,8 @@
  * TEST INFRASTRUCTURE ONLY (see oracle.h).  Plain C99, single-threaded, FP64,
  * written to follow the reference's arithmetic order where the reference has
  * code, and extended from 2D to 3D where it does not.  Every function names
- * the reference lines it restates.  Deviations from the reference (each one
- * listed in DESIGN.md):
+ * the reference lines it restates.  Deviations from the reference, each
+ * with its reason:
  *   D1 ell_set_zero_col returns at the first -1 slot of any row
  *      (src/ell.c:103-118): orc_ell_set_zero_col_ref keeps that behaviour,
  *      orc_ell_set_zero_col_full zeroes the column in every row (needed for a
