@@ -4,9 +4,10 @@ Workload (one "step"): 4096 independent micro-RVEs, structured hex8 meshes
 with n drawn uniformly from {8, 12, 16, 20} elements per edge, a centred
 z-aligned fiber of radius U(0.1, 0.35), matrix E = 1e9 Pa, fiber/matrix
 stiffness ratio log-uniform in [2, 100], Poisson ratios U(0.2, 0.35); each RVE
-is assembled, solved for its 6 unit-strain load cases to a 1e-8 relative FP64
-residual and volume-averaged (the 6x6 homogenized tangent).  One persistent
-launch per step, FP32 ELL values and CG with FP64 residual refinement.
+is solved for its 6 unit-strain load cases to a 1e-8 relative FP64 residual
+and volume-averaged (the 6x6 homogenized tangent).  One persistent launch per
+step: FP32 Jacobi-PCG on the matrix-free element-type stencil (or, with
+--op ell, on assembled FP32 ELL values) with FP64 residual refinement.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 

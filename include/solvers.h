@@ -4,8 +4,11 @@
  *
  * The solver selector stays as it is.  SOLVER_ELL_GPU is new: it names the
  * ELL Jacobi-PCG of libsputnik_b200.so.  The PETSc KSP printer
- * (inc/solvers.h:15-18) exists only when the caller builds with PETSc, as in
- * the reference; this library has no PETSc dependency.
+ * (inc/solvers.h:15-18) exists only when the caller builds with PETSc, and
+ * the SLEPc include (inc/solvers.h:20-22) only when it builds with SLEPc, as
+ * in the reference: the macro program is compiled with -DSLEPC and reaches
+ * its EPS type through this header (macro/inc/macro.h:12).  This library
+ * itself has no PETSc or SLEPc dependency.
  */
 #ifndef SOLVERS_H
 #define SOLVERS_H
@@ -35,6 +38,10 @@ extern solver_t solver;
 #ifdef PETSC
 #include "petscksp.h"
 int solvers_print_petsc_ksp_info(MPI_Comm COMM, KSP ksp);
+#endif
+
+#ifdef SLEPC
+#include "slepceps.h"
 #endif
 
 #endif

@@ -88,17 +88,22 @@ int sp_ell_dev_pcg(sp_ell_dev *a, const double *b, double *x, double rtol, int m
 /* Jacobi-preconditioned CG (the algorithm of sp_ell_dev_pcg) on an ELL
  * matrix the caller already holds in device memory, allocating nothing.
  * No counterpart in the reference: it is for callers that cannot allocate
- * device memory -- code running during CUDA stream capture (where cudaMalloc
- * is not allowed), latency-bound loops that must stay out of the allocator,
- * and frameworks that own all device memory through their own pool.
- * cols_dev/vals_dev: [nrow][nnz] row-major, -1 ends a row (the ell.h layout);
- * b_dev: right-hand side; x_dev: initial guess in, solution out; all device
- * pointers owned by the caller.  Stops at ||b - A x|| <= rtol ||b||.
- * Work space is a fixed device array of the library (about 8.4 MB per GPU,
- * held until exit): nrow <= SP_NOALLOC_MAX_ROWS, else SP_ERR_ARG.  The first
- * call on a device looks up that array's address; make it before any stream
- * capture.  Calls share the array: calls that overlap on the GPU race, so
- * serialize them.  stream NULL means the per-thread default stream. */
+ * device memory -- frameworks that own all device memory through their own
+ * pool and forbid other allocations, and latency-bound loops that must stay
+ * out of the CUDA allocator (whose calls synchronize the device).
+ * cols_dev/vals_dev: [nrow][nnz] row-major, -1 marks an empty slot (the ell.h
+ * layout); b_dev: right-hand side; x_dev: initial guess in, solution out; all
+ * device pointers owned by the caller.  Stops at ||b - A x|| <= rtol ||b||.
+ * Returns SP_ERR_RANGE for a column index outside [0, nrow) (the entry is
+ * skipped, never read), SP_ERR_ARG for a row whose diagonal is zero or
+ * absent, SP_ERR_NOCONV when the residual test fails (including a NaN
+ * residual).  Work space is a fixed device array of the library (about
+ * 8.4 MB per GPU, held until exit): nrow <= SP_NOALLOC_MAX_ROWS, else
+ * SP_ERR_ARG.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress); make it before any stream capture.  Calls share
+ * the array and each call resets what must start at zero; calls that
+ * overlap on the GPU race, so serialize them.  stream NULL means the
+ * per-thread default stream. */
 #define SP_NOALLOC_MAX_ROWS 262144
 int sp_ell_pcg_noalloc(int nrow, int nnz, const int *cols_dev, const double *vals_dev,
                        const double *b_dev, double *x_dev, double rtol, int max_its, int *its,

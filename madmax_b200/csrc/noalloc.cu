@@ -2,19 +2,21 @@
 // matrix that already lives in device memory, for callers that cannot
 // allocate device memory.
 //
-// Who needs it: code that runs while a CUDA stream is being captured into a
-// graph (cudaMalloc is not allowed during capture), latency-bound serving
-// loops that must never enter the allocator, and host frameworks that hand
-// out all device memory from their own pool and forbid other allocations.
-// Such a caller passes its matrix and vectors as device pointers it
-// already owns; this entry point calls no cudaMalloc, cudaFree or other
-// allocating routine.  Its work space (diagonal inverse, three CG vectors,
-// reduction partials, scalars) is one file-scope __device__ array of fixed
-// size, so at most SP_NOALLOC_MAX_ROWS rows fit.
+// Who needs it: host frameworks that hand out all device memory from their
+// own pool and forbid allocations behind their back, and latency-bound
+// serving loops that must never enter the CUDA allocator (cudaMalloc and
+// cudaFree synchronize the device and can stall for milliseconds).  Such a
+// caller passes its matrix and vectors as device pointers it already owns;
+// this entry point calls no cudaMalloc, cudaFree or other allocating
+// routine.  Its work space (diagonal inverse, three CG vectors, reduction
+// partials, scalars) is one file-scope __device__ array of fixed size, so at
+// most SP_NOALLOC_MAX_ROWS rows fit.
 //
 // Set-up: the first call on a device, with that device current, looks up
-// the array's device address with cudaGetSymbolAddress and keeps it for
-// later calls.  Make that first call before any stream capture begins.
+// the array's device address with cudaGetSymbolAddress and keeps it; later
+// calls check that the kept address is still a device address of that
+// device (after a cudaDeviceReset it is not) and look it up again if not.
+// Make the first call on a device before any stream capture begins.
 //
 // The array is shared by every call on a device and keeps the contents of
 // the last call; each call clears what must start at zero.  Two calls whose
@@ -35,9 +37,12 @@ constexpr int MAX_BLOCKS = 1024;
 struct State {
   double rho, alpha, beta, bb, rr;
   double rtol2;
-  int its, max_its, active, bad;
+  int its, max_its, active;
+  int bad;    // a column index outside [0, nrow) other than -1
+  int zdiag;  // a row whose diagonal is zero or absent
   unsigned ticket;
 };
+static_assert(sizeof(State) <= 32 * sizeof(double), "State fits its slot of the work space");
 
 // layout of the scratch array (doubles)
 constexpr size_t OFF_STATE = 0;                                // State (padded to 32 doubles)
@@ -65,6 +70,18 @@ __device__ inline double warp_row(int row, int n, int nnz, const int *cols, cons
   }
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
   return s;
+}
+
+// The diagonal entry of a row (the sum of its slots in column row; 0 when
+// there is none), by the whole warp; slots of -1 are skipped wherever they
+// are, as warp_row skips them.
+__device__ inline double warp_diag(int row, int nnz, const int *cols, const double *vals,
+                                   int lane) {
+  double d = 0.0;
+  for (int j = lane; j < nnz; j += 32)
+    if (cols[(size_t)row * nnz + j] == row) d += vals[(size_t)row * nnz + j];
+  for (int off = 16; off > 0; off >>= 1) d += __shfl_xor_sync(0xffffffffu, d, off);
+  return d;
 }
 
 // Last-arriving block folds the per-block partials (3 per block) in block
@@ -118,14 +135,10 @@ __global__ void __launch_bounds__(THREADS)
   double rz = 0.0, bb = 0.0, rr = 0.0;
   for (int row = warp; row < n; row += nw) {
     double ax = warp_row(row, n, nnz, cols, vals, x, lane, &st->bad);
-    double diag = 0.0;
-    for (int j = 0; j < nnz; j++) {
-      int c = cols[(size_t)row * nnz + j];
-      if (c < 0) break;
-      if (c == row) diag = vals[(size_t)row * nnz + j];
-    }
+    double diag = warp_diag(row, nnz, cols, vals, lane);
     if (lane == 0) {
-      double di = 1.0 / diag, rv = b[row] - ax, z = di * rv;
+      if (!(diag != 0.0)) st->zdiag = 1;  // zero, absent or NaN: no Jacobi inverse
+      double di = (diag != 0.0) ? 1.0 / diag : 0.0, rv = b[row] - ax, z = di * rv;
       dinv[row] = di;
       r[row] = rv;
       p[row] = z;
@@ -140,7 +153,8 @@ __global__ void __launch_bounds__(THREADS)
     st->bb = tot[1];
     st->rr = tot[2];
     st->its = 0;
-    st->active = tot[1] > 0.0 && st->max_its > 0 && tot[2] > st->rtol2 * tot[1] && !st->bad;
+    st->active = tot[1] > 0.0 && st->max_its > 0 && tot[2] > st->rtol2 * tot[1] && !st->bad &&
+                 !st->zdiag && isfinite(tot[0]) && isfinite(tot[1]) && isfinite(tot[2]);
   }
 }
 
@@ -185,7 +199,9 @@ __global__ void __launch_bounds__(THREADS) k_update(int n, double *x, double *S)
   if (fold3(rz, rr, 0.0, S + OFF_PART, &st->ticket, tot)) {
     st->rr = tot[1];
     st->its++;
-    if (tot[1] <= st->rtol2 * st->bb || st->its >= st->max_its || st->bad) {
+    // a NaN or infinite residual is a breakdown: stop (the host reports it)
+    if (tot[1] <= st->rtol2 * st->bb || st->its >= st->max_its || st->bad || !isfinite(tot[0]) ||
+        !isfinite(tot[1])) {
       st->active = 0;
       st->beta = 0.0;
     } else {
@@ -209,10 +225,22 @@ __global__ void __launch_bounds__(THREADS) k_dir(int n, double *S) {
 static std::mutex g_mu;
 static double *g_addr[64];
 
-// once per device, with that device current
+// whether p is still a device address of device dev (after a
+// cudaDeviceReset the kept address belongs to a destroyed context)
+static bool still_device_address(const double *p, int dev) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
+// the work space's device address, looked up once per device with that
+// device current, and again when the kept one is no longer valid
 static int scratch_address(int dev, double **out) {
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
+  if (!g_addr[dev] || !still_device_address(g_addr[dev], dev)) {
     double *ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_scratch);
     if (e != cudaSuccess)
@@ -274,10 +302,16 @@ extern "C" int sp_ell_pcg_noalloc(int nrow, int nnz, const int *cols_dev, const 
     SP_CUDA_TRY(cudaStreamSynchronize(s));
   }
   if (its) *its = st.its;
-  if (relres) *relres = (st.bb > 0) ? sqrt(st.rr / st.bb) : 0.0;
+  if (relres) *relres = (st.bb > 0) ? sqrt(st.rr / st.bb) : (st.bb == 0.0 ? 0.0 : NAN);
   if (st.bad)
     return sp_set_error(SP_ERR_RANGE, "sp_ell_pcg_noalloc: column index outside [0, nrow)");
-  if (st.bb > 0 && st.rr > st.rtol2 * st.bb)
-    return sp_set_error(SP_ERR_NOCONV, "sp_ell_pcg_noalloc: no convergence in %d its", st.its);
+  if (st.zdiag)
+    return sp_set_error(SP_ERR_ARG, "sp_ell_pcg_noalloc: a row has a zero or no diagonal entry");
+  // success only when the residual test holds (false for NaN): b = 0 is
+  // solved by x = 0 only if the start iterate is 0
+  const bool conv = (st.bb == 0.0) ? (st.rr == 0.0) : (st.rr <= st.rtol2 * st.bb);
+  if (!conv)
+    return sp_set_error(SP_ERR_NOCONV, "sp_ell_pcg_noalloc: no convergence in %d its (residual %g)",
+                        st.its, st.bb > 0 ? sqrt(st.rr / st.bb) : sqrt(st.rr));
   return SP_OK;
 }

@@ -5,11 +5,17 @@
 // runs the whole micro solve of micro/src/homogenize.c:175-225 for all load
 // cases of that RVE on its own:
 //   1. element operators (D, Ke = sum B^T D B w, Bbar) in shared memory;
-//   2. assembly: the RVE's ELL values by the 8-colour conflict-free scatter,
-//      then Dirichlet rows/columns and the Jacobi diagonal;
-//   3. refinement loop: FP64 residual b = -K u from the element operators
-//      (the FP64 "true" residual), FP32 Jacobi-PCG on the ELL values for the
-//      correction A x = b, u += x in FP64, until ||b_k|| <= rtol ||b_k,0||;
+//   2. the inner operator: by default (SP_OP_STENCIL) no matrix at all --
+//      the element-type stencil reads the node's 27 neighbour blocks from a
+//      table of the two materials' element blocks in shared memory, and only
+//      the Jacobi diagonal is formed; with SP_OP_ELL the RVE's FP32 ELL
+//      values are assembled by the 8-colour conflict-free scatter, with
+//      Dirichlet rows/columns, into a node-sliced copy;
+//   3. refinement loop: FP64 residual b = -K u from the FP64 element
+//      operators (the "true" residual), FP32 Jacobi-PCG on the inner
+//      operator for the correction A x = b (reliable updates: the search
+//      direction carries over between corrections), u += x in FP64, until
+//      ||b_k|| <= rtol ||b_k,0||;
 //   4. FP64 volume averages of strain and stress per load case.
 // A CTA never waits on another CTA, so the kernel needs no grid barrier and
 // no co-residency guarantee.  All reductions are CTA-local and deterministic:

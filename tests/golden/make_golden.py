@@ -17,7 +17,7 @@ the tests never need it):
   4. readme_2d.json  -- the 2D homogenized tensor printed in exs/README.md:
      154-157, with the run parameters.
 
-    python tests/golden/make_golden.py
+    REF_DIR=<reference checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -35,7 +35,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 
-REF_DIR = "/root/reference"
+# the reference checkout the fixtures are generated from (required)
+REF_DIR = os.environ.get("REF_DIR", "")
 
 
 def hexs(a):
@@ -175,8 +176,9 @@ def readme_2d():
 
 
 def main():
-    if not os.path.isdir(REF_DIR):
-        sys.exit("reference tree not present; fixtures are committed")
+    if not REF_DIR or not os.path.isdir(REF_DIR):
+        sys.exit("set REF_DIR to the reference checkout (the fixtures are committed)")
+    os.environ["REF_DIR"] = REF_DIR
     O.build()
     json.dump(unity_ell(), open(os.path.join(HERE, "unity_ell.json"), "w"), indent=1)
     fem_tables()

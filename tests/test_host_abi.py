@@ -235,3 +235,28 @@ def test_public_headers_compile_standalone(tmp_path, compiler, std):
                             "-I", os.path.join(ROOT, "include"), str(src)],
                            capture_output=True, text=True)
         assert r.returncode == 0, (h, r.stderr[-2000:])
+
+
+def test_solvers_header_includes_slepc_under_dslepc(tmp_path):
+    """The macro program is built with -DSLEPC and declares its EPS solver
+    through solvers.h (inc/solvers.h:20-22, macro/inc/macro.h:12): with
+    -DSLEPC the header pulls in slepceps.h, found first on the caller's
+    include path (here a stub that defines EPS)."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("gcc not found")
+    stub = tmp_path / "stub"
+    stub.mkdir()
+    (stub / "slepceps.h").write_text("typedef struct sp_stub_eps *EPS;\n")
+    src = tmp_path / "macro_like.c"
+    src.write_text('#include "solvers.h"\nEPS eps;\nsolver_t solver;\n'
+                   "int sp_probe(void) { return eps == 0 && solver.type == SOLVER_NULL; }\n")
+    inc = ["-I", os.path.join(ROOT, "include"), "-I", str(stub)]
+    ok = subprocess.run(["gcc", "-std=gnu11", "-Wall", "-Werror", "-DSLEPC", "-fsyntax-only"] +
+                        inc + [str(src)], capture_output=True, text=True)
+    assert ok.returncode == 0, ok.stderr[-2000:]
+    # without -DSLEPC the stub is not included, so EPS is unknown
+    no = subprocess.run(["gcc", "-std=gnu11", "-fsyntax-only"] + inc + [str(src)],
+                        capture_output=True, text=True)
+    assert no.returncode != 0 and "EPS" in no.stderr
