@@ -101,22 +101,29 @@ def argv_tail(args):
             f"--inner-rtol {args.inner_rtol:g}"]
 
 
-def profiled_traffic(name: str, workload: str):
-    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
-    from the committed ncu summary profiles/<name>, when its `workload:`
-    line names this run's workload; None otherwise."""
-    path = os.path.join(ROOT, "profiles", name)
-    try:
-        txt = open(path).read()
-    except OSError:
-        return None
-    wl = tb = None
-    for line in txt.splitlines():
-        if line.startswith("workload: "):
-            wl = line[len("workload: "):].strip().strip("`")
-        if line.startswith("traffic_bytes_per_launch: "):
-            tb = int(line.split(":")[1])
-    return tb if wl == workload and tb else None
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one ncu capture of exactly these workloads; the command of each capture is
+# in the summary under profiles/ named for its kernel and workload.  The
+# bench cannot count DRAM bytes itself, so a run whose workload differs
+# reports null.
+PROFILED_TRAFFIC = {
+    # k_batch, stencil operator: ncu --metrics dram__bytes_read.sum,
+    # dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
+    # -k regex:k_batch -s 3 -c 1 python bench.py --steps 1 --warmup 3 ...
+    "k_batch --nrve 4096 --sizes 8 12 16 20 --op stencil --threads 0 --ctas 0 "
+    "--inner-rtol 0.0001": 1039010537728,
+    # k_spmv_rve, the n = 40 structured matrix, cold L2
+    "k_spmv_rve structured ELL n=40": 218744832,
+}
+
+
+def profiled_traffic(kernel: str, workload: str):
+    """(bytes per launch, source) of the ncu capture of this workload, or
+    (None, reason) when none was taken of it."""
+    tb = PROFILED_TRAFFIC.get(f"{kernel} {workload}")
+    if tb is None:
+        return None, "no ncu capture of this workload"
+    return tb, "ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum)"
 
 
 def structured_ell(n: int, seed: int = 5):
@@ -145,9 +152,10 @@ def structured_ell(n: int, seed: int = 5):
 
 def measure_spmv(mb, stream, sptr, n=40, reps=20):
     """The resident FP64 ELL SpMV (sp_ell_dev_mvp) on one matrix larger than
-    L2, L2 flushed before every launch, at every lanes-per-row setting;
-    achieved = algorithmic bytes (stored slots x 12 + x read + y write) /
-    CUDA-event time per launch."""
+    L2, at the lanes-per-row width the library's upload-time autotuner chose
+    (no override), L2 flushed before every timed launch; achieved =
+    algorithmic bytes (stored slots x 12 + x read + y write) / CUDA-event
+    time per launch."""
     import torch
     cols, vals = structured_ell(n)
     m = mb.ell_matrix()
@@ -160,6 +168,9 @@ def measure_spmv(mb, stream, sptr, n=40, reps=20):
     try:
         nrow, wp, nnz = C.c_int(), C.c_int(), C.c_longlong()
         mb.check(mb.lib().sp_ell_dev_info(h, C.byref(nrow), C.byref(wp), C.byref(nnz)), "info")
+        lanes, cached = C.c_int(), C.c_int()
+        trial = (C.c_float * 4)()
+        mb.check(mb.lib().sp_ell_dev_lanes(h, C.byref(lanes), trial, C.byref(cached)), "lanes")
         x_h = np.random.default_rng(6).standard_normal(nrow.value)
         x = torch.from_numpy(x_h).cuda()
         y = torch.empty_like(x)
@@ -176,34 +187,33 @@ def measure_spmv(mb, stream, sptr, n=40, reps=20):
         # lines, so no write-back of the flush lands inside the timing)
         flush = torch.ones(64 << 20, dtype=torch.float32, device="cuda")
         sink = torch.empty(1, dtype=torch.float32, device="cuda")
-        per = {}
-        for lanes in (4, 8, 16, 32):
-            mb.check(mb.lib().sp_ell_dev_set_lanes(h, lanes), "lanes")
-            for _ in range(3):
-                mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr)
-            evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                   for _ in range(reps)]
-            torch.cuda.synchronize()
-            for e0, e1 in evs:
-                torch.sum(flush, dim=0, out=sink[0])
-                e0.record(stream)
-                mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr)
-                e1.record(stream)
-            torch.cuda.synchronize()
-            per[lanes] = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
+        for _ in range(3):
+            mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(reps)]
+        torch.cuda.synchronize()
+        for e0, e1 in evs:
+            torch.sum(flush, dim=0, out=sink[0])
+            e0.record(stream)
+            mb.lib().sp_ell_dev_mvp(h, xp, yp, sptr)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / reps
         del flush, sink
-        best = min(per, key=per.get)
         abytes = nnz.value * 12 + 2 * nrow.value * 8
         peak, peak_kind = measured_peak()
-        ach = abytes / (per[best] / 1e3) / 1e9
+        ach = abytes / (ms / 1e3) / 1e9
         return {"kernel": "k_spmv_rve (sp_ell_dev_mvp, FP64 ELL, hoisted loads)",
                 "matrix": f"hex8 RVE sparsity n={n}: {nrow.value} rows x 84 slots, "
                           f"{nnz.value} stored, {(vals.nbytes + cols.nbytes) / 1e6:.0f} MB > L2",
                 "l2": "flushed before every timed launch (a 256 MB read)",
-                "lanes_per_row": best, "ms": per[best],
-                "ms_by_lanes": {str(k): round(v, 4) for k, v in per.items()},
-                "algorithmic_bytes": abytes,
-                "traffic": profiled_traffic("k_spmv_rve_n40_fp64.md", f"structured ELL n={n}"),
+                "lanes_per_row": lanes.value,
+                "lanes_source": "the library's upload-time autotuner" +
+                                (" (cached choice)" if cached.value else ""),
+                "autotuner_trial_us": {str(w): round(float(t), 2)
+                                       for w, t in zip((4, 8, 16, 32), trial)},
+                "ms": ms, "algorithmic_bytes": abytes,
+                "traffic": profiled_traffic("k_spmv_rve", f"structured ELL n={n}")[0],
                 "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_kind": peak_kind, "max_rel_err_vs_numpy": err}
     finally:
@@ -338,6 +348,30 @@ def workload_config(args, sizes):
             "nrve_per_gpu": args.nrve, "load_cases": 6, "rtol": 1e-8}
 
 
+def oracle_check(descs, stress, per_size: int, seed: int = 31):
+    """Per-RVE error of the timed batch's stresses against the FP64 oracle
+    (relative residual 1e-12) on a seeded sample of the mix, `per_size` RVEs
+    of every mesh size: |sigma - sigma_oracle|max / |sigma_oracle|max over the
+    6 unit-strain load cases of each RVE."""
+    from oracle import pool as OP
+    rng = np.random.default_rng(seed)
+    picked = []
+    for s_ in sorted(set(int(d.n[0]) for d in descs)):
+        idx = [i for i, d in enumerate(descs) if d.n[0] == s_]
+        picked += sorted(rng.choice(idx, size=min(per_size, len(idx)), replace=False).tolist())
+    items = [(int(descs[i].n[0]), descs[i].radius, (descs[i].E[0], descs[i].E[1]),
+              (descs[i].nu[0], descs[i].nu[1]), np.eye(6)) for i in picked]
+    t0 = time.perf_counter()
+    want = OP.run(OP.homogenize, items)
+    errs = [float(np.abs(stress[i] - w).max() / np.abs(w).max()) for i, w in zip(picked, want)]
+    return {"rves": len(picked), "per_size": per_size, "max": max(errs),
+            "p99": float(np.percentile(errs, 99)), "median": float(np.median(errs)),
+            "per_rve": [{"rve": int(i), "n": int(descs[i].n[0]), "err": e}
+                        for i, e in zip(picked, errs)],
+            "oracle": "FP64 Jacobi-PCG restatement, relative residual 1e-12",
+            "oracle_s": time.perf_counter() - t0}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -404,6 +438,7 @@ def run_ours(args):
                      op=mb.SP_OP_STENCIL if args.op == "stencil" else mb.SP_OP_ELL)
     setup_s = time.time() - t0
     shape = batch.shape()
+    tuned = batch.tune_report()
 
     for _ in range(args.warmup):
         batch.launch(sptr)
@@ -464,6 +499,7 @@ def run_ours(args):
     line = None
     if rank == 0:
         abytes = algorithmic_bytes(sizes, inf["inner"], inf["outer"], stencil=args.op == "stencil")
+        traffic, traffic_src = profiled_traffic("k_batch", " ".join(argv_tail(args)))
         avg_ms = total_ms / args.steps
         achieved = abytes / (avg_ms / 1000.0) / 1e9
         peak, peak_kind = measured_peak()
@@ -476,6 +512,7 @@ def run_ours(args):
                        "precision": "mixed", "cta_threads": shape[0], "ctas_per_sm": shape[1],
                        "persistent_grid": shape[2],
                        "cluster": args.cluster, "inner_rtol": args.inner_rtol,
+                       "shape_source": "autotuner" if tuned else "given",
                        "operator": args.op,
                        "l2": l2_note(args, sizes, batch),
                        "parallelism": f"replicas x{world} (independent RVEs per rank)"},
@@ -484,21 +521,33 @@ def run_ours(args):
             "gpu_launches": args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
-                         "traffic": profiled_traffic("k_batch_stencil_4096rve_traffic.md",
-                                                     " ".join(argv_tail(args))),
+                         "traffic": traffic, "traffic_source": traffic_src,
                          "algorithmic_bytes": abytes,
                          "peak_kind": peak_kind, "kernel": "k_batch (persistent)"},
             "clocks": clocks,
+            "converged": converged, "max_relres": float(inf["relres"].max()),
+            "autotuner": tuned,
             "solve": {"converged": converged, "max_relres": float(inf["relres"].max()),
                       "mean_inner_its": float(inf["inner"].mean()),
                       "mean_outer_its": float(inf["outer"].mean()),
                       "rhs_solves_per_s": 6 * value, "setup_s": setup_s},
         }
+        if world == 1 and args.oracle_sample > 0:
+            oc = oracle_check(descs, stress, args.oracle_sample)
+            line["oracle_err"] = oc
+            line["oracle_err_max"] = oc["max"]
+            line["oracle_err_p99"] = oc["p99"]
         if world == 1 and not args.no_spmv:
             line["spmv"] = measure_spmv(mb, stream, sptr)
         if world == 1 and not args.no_plain:
             line["plain_gpu"] = plain_gpu(mb, descs, args)
             line["plain_gpu"]["batched_speedup"] = value / line["plain_gpu"]["value"]
+            line["batched_speedup"] = line["plain_gpu"]["batched_speedup"]
+        if world == 1 and not args.no_ell:
+            line["ell_batch"] = ell_batch(mb, descs, args, stream, sptr)
+            if "plain_gpu" in line:
+                line["ell_batch"]["batched_speedup"] = (line["ell_batch"]["value"] /
+                                                        line["plain_gpu"]["value"])
         if world == 1 and not args.no_serve:
             line["serving"] = serving(mb, args)
         if world == 1 and not args.no_fe2:
@@ -534,112 +583,194 @@ def fe2_step(mb, args):
     """A full FE2 step: 40x10x10 hex8 cantilever (14,883 dof, 32,000 Gauss
     points), tip traction 1e6 Pa, every Gauss point bound to one of 64
     seeded RVEs (n = 16, fibre radius U(0.15, 0.3), matrix E 1e9 nu 0.3,
-    fibre E 1e10 nu 0.2), 5 Newton iterations, FP64 macro solve; the micro
-    tangents come from the serving loop."""
+    fibre E 1e10 nu 0.2), FP64 macro solve; micro answers from the serving
+    loop.  Three runs: the linear micro mode (one FD tangent per RVE, the
+    reference micro's own behaviour for linear materials) with the
+    reference's 1e-6 strain clip, the same without the clip, and one serving
+    request per Gauss point per Newton iteration (32,000 per iteration)."""
     rng = np.random.default_rng(5150)
     rves = [mb.rve_desc(16, float(rng.uniform(0.15, 0.3)), (1e9, 1e10), (0.3, 0.2))
             for _ in range(64)]
-    t0 = time.perf_counter()
-    f = mb.Fe2(rves, newton_its=5)
-    setup = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    info = f.run()
-    step = time.perf_counter() - t0
-    f.close()
-    out = {"macro": "40x10x10 hex8 cantilever, 14883 dof, 32000 Gauss points, traction 1e6 Pa",
-           "rves": "64 x n=16 (seeded)", "micro": "linear: FD tangent around zero per RVE",
-           "micro_setup_s": setup, "step_s": step, "newton_its": info.newton_its,
-           "bnorm": [info.bnorm[i] for i in range(info.newton_its)],
-           "pcg_its": [info.pcg_its[i] for i in range(info.newton_its)],
-           "tip_displacement": list(info.tip), "micro_requests": info.micro_requests,
-           "device_ms": {"residual": info.residual_ms, "assemble": info.assemble_ms,
-                         "solve": info.solve_ms}}
-    if args.fe2_per_gp:
-        # iteration 1 sees zero strains everywhere (answered from the warm
-        # starts); iteration 2 solves 32,000 distinct strains
+
+    def one(label, its, **kw):
         t0 = time.perf_counter()
-        g = mb.Fe2(rves, newton_its=2, micro=mb.SP_FE2_PER_GP)
-        gi = g.run()
-        out["per_gauss_point"] = {"newton_its": 2, "requests": gi.micro_requests,
-                                  "micro_s": gi.micro_s, "total_s": time.perf_counter() - t0,
-                                  "requests_per_s": gi.micro_requests / gi.micro_s,
-                                  "tip_displacement": list(gi.tip)}
-        g.close()
+        f = mb.Fe2(rves, newton_its=its, **kw)
+        setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        info = f.run()
+        step = time.perf_counter() - t0
+        f.close()
+        bn = [info.bnorm[i] for i in range(info.newton_its)]
+        r = {"mode": label, "newton_its": info.newton_its, "setup_s": setup, "step_s": step,
+             "bnorm": bn, "final_rel_residual": bn[-1] / bn[0],
+             "pcg_its": [info.pcg_its[i] for i in range(info.newton_its)],
+             "tip_displacement": list(info.tip), "micro_requests": info.micro_requests,
+             "device_ms": {"residual": info.residual_ms, "assemble": info.assemble_ms,
+                           "solve": info.solve_ms}}
+        if info.micro_s > 0:
+            r["micro_s"] = info.micro_s
+            r["micro_requests_per_s"] = info.micro_requests / info.micro_s
+        return r
+
+    # without the clip the loop converges; it stops once ||b|| <= 1e-6 N (1e-11
+    # of the first residual), since a right-hand side at the round-off level
+    # of the internal forces cannot be reduced by the macro PCG's relative
+    # tolerance
+    tol = 1e-6
+    out = {"macro": "40x10x10 hex8 cantilever, 14883 dof, 32000 Gauss points, traction 1e6 Pa",
+           "rves": "64 x n=16 (seeded)",
+           "linear_clip": one("linear micro, strain clip 1e-6 (macro/src/assembly.c:319)", 5),
+           "linear_noclip": one("linear micro, no strain clip", 5, strain_clip=0.0,
+                                newton_tol=tol)}
+    if not args.no_fe2_per_gp:
+        out["per_gauss_point"] = one("one serving request per Gauss point per iteration, "
+                                     "no strain clip", 5, micro=mb.SP_FE2_PER_GP,
+                                     strain_clip=0.0, newton_tol=tol)
     return out
 
 
-def serving(mb, args):
-    """Open-loop Poisson load on the device-resident server; the plain path
-    is one FIFO server whose service times are measured per geometry with
-    the plain FP64 solve of the same 7 load cases."""
-    import torch
-    geoms = serve_geometries(mb, args.serve_geoms, 4321)
-    t0 = time.time()
-    srv = mb.Server(geoms, hbm_budget=150 * 10 ** 9)
-    setup = time.time() - t0
-    srv.start()
-    rng = np.random.default_rng(99)
-    # first request on every geometry: a cold solve (no warm start yet)
-    warm_g = np.arange(len(geoms))
-    td0, _, _, info0 = srv.replay(warm_g, rng.normal(0, 1e-3, (len(geoms), 6)),
-                                  np.zeros(len(geoms)), timeout=600)
-    out = {"geometries": len(geoms), "n_range": [8, 32], "setup_s": setup,
-           "cold_first_pass": {"requests": len(geoms), "seconds": float(td0.max()),
-                               "solves_per_s": len(geoms) / float(td0.max()),
-                               "mean_inner_its": float(np.mean([i.inner_its for i in info0]))},
-           "warm_start": "first-order prediction from the geometry's last solved request, "
-                         "verified by the FP64 residual; requests that miss 1e-8 are solved",
-           "rates": {}}
-    plain_samples = {}
+def serve_traces(args, ngeom: int, seed: int = 99):
+    """Poisson traces, one per arrival rate: (rate, arrival times, geometry
+    ids, strains N(0, 1e-3))."""
+    rng = np.random.default_rng(seed)
+    out = []
     for lam in args.serve_rates:
         nreq = int(min(args.serve_max_req, max(200, lam * args.serve_seconds)))
         t_arr = np.cumsum(rng.exponential(1.0 / lam, size=nreq))
-        geo = rng.integers(0, len(geoms), size=nreq)
-        eps = rng.normal(0, 1e-3, size=(nreq, 6))
+        out.append((lam, t_arr, rng.integers(0, ngeom, size=nreq),
+                    rng.normal(0, 1e-3, size=(nreq, 6))))
+    return out
+
+
+def serve_mode(mb, geoms, traces, warm_start):
+    """One server over the resident geometries: a cold first request on every
+    geometry, then every trace replayed open-loop (arrivals on the host clock,
+    completion times from the done flags)."""
+    t0 = time.time()
+    srv = mb.Server(geoms, hbm_budget=150 * 10 ** 9, warm_start=warm_start)
+    setup = time.time() - t0
+    srv.start()
+    rng = np.random.default_rng(7)
+    g0 = np.arange(len(geoms))
+    td0, _, _, info0 = srv.replay(g0, rng.normal(0, 1e-3, (len(geoms), 6)), np.zeros(len(geoms)),
+                                  timeout=600)
+    out = {"setup_s": setup,
+           "cold_first_pass": {"requests": len(geoms), "seconds": float(td0.max()),
+                               "solves_per_s": len(geoms) / float(td0.max()),
+                               "mean_inner_its": float(np.mean([i.inner_its for i in info0]))},
+           "rates": {}}
+    for lam, t_arr, geo, eps in traces:
         td, st, tg, info = srv.replay(geo, eps, t_arr, timeout=900)
         lat = (td - t_arr) * 1000.0
-        ok = all(i.status == 0 for i in info)
         span = td.max() - t_arr.min()
-        out["rates"][str(lam)] = {"requests": nreq, "p50_ms": float(np.percentile(lat, 50)),
-                                  "p99_ms": float(np.percentile(lat, 99)),
-                                  "solves_per_s": nreq / span, "all_converged": ok,
-                                  "solved_fraction": float(np.mean([i.outer_its > 0 for i in info])),
-                                  "max_relres": float(max(i.relres for i in info))}
-        plain_samples[lam] = (t_arr, geo)
+        out["rates"][str(lam)] = {
+            "requests": len(t_arr), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": len(t_arr) / span,
+            "all_converged": all(i.status == 0 for i in info),
+            "solved_fraction": float(np.mean([i.outer_its > 0 for i in info])),
+            "mean_inner_its": float(np.mean([i.inner_its for i in info])),
+            "max_relres": float(max(i.relres for i in info))}
     srv.stop()
     srv.close()
-    # plain: service time per geometry (7 load cases, FP64, one RVE at a time)
-    sizes = sorted(set(int(g.n[0]) for g in geoms))
-    probe = [s for s in sizes if s in (8, 14, 20, 26, 32)] or sizes[:3]
-    svc = {}
-    for sz in probe:
-        d = next(g for g in geoms if g.n[0] == sz)
-        r = mb.Rve(d)
-        e = np.tile(rng.normal(0, 1e-3, 6), (7, 1))
-        for i in range(6):
-            e[i + 1, i] += 0.005
-        r.homogenize(e)
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        r.homogenize(e)
-        svc[sz] = time.perf_counter() - t
-        r.close()
-    xs = np.array(sorted(svc))
-    ys = np.array([svc[k] for k in xs])
-    for lam, (t_arr, geo) in plain_samples.items():
-        service = np.interp([geoms[g].n[0] for g in geo], xs, ys)
-        free = 0.0
-        lat = np.zeros(len(t_arr))
-        for i, (ta, sv) in enumerate(zip(t_arr, service)):
-            start = max(ta, free)
-            free = start + sv
-            lat[i] = (free - ta) * 1000.0
-        span = free - t_arr.min()
-        out["rates"][str(lam)]["plain"] = {"p50_ms": float(np.percentile(lat, 50)),
-                                           "p99_ms": float(np.percentile(lat, 99)),
-                                           "solves_per_s": len(t_arr) / span}
-    out["plain_service_s"] = {str(k): float(v) for k, v in svc.items()}
     return out
+
+
+def plain_replay(mb, geoms, trace, nreq: int):
+    """The plain comparator, run for real: the first `nreq` requests of a
+    trace served one at a time in arrival order by the plain FP64 path
+    (sp_rve_homogenize on the geometry's resident ELL matrix, the request's 7
+    load cases eps and eps + 0.005 e_i, cold start).  Every geometry the
+    sample uses is created and solved once before the replay (resident and
+    warm, like the server's); each request starts at max(arrival, previous
+    completion) on the host clock."""
+    import torch
+    lam, t_arr, geo, eps = trace
+    t_arr, geo, eps = t_arr[:nreq], geo[:nreq], eps[:nreq]
+    rves = {}
+    e7 = lambda e: np.vstack([e] + [e + 0.005 * np.eye(6)[i] for i in range(6)])
+    for g in sorted(set(int(x) for x in geo)):
+        rves[g] = mb.Rve(geoms[g])
+        rves[g].homogenize(e7(np.zeros(6)))
+    torch.cuda.synchronize()
+    done = np.zeros(len(t_arr))
+    ok = True
+    t0 = time.perf_counter()
+    for i in range(len(t_arr)):
+        wait = t0 + t_arr[i] - t_arr[0] - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        _, _, _, info = rves[int(geo[i])].homogenize(e7(eps[i]))
+        ok = ok and info.status == 0
+        done[i] = time.perf_counter() - t0
+    for r in rves.values():
+        r.close()
+    lat = (done - (t_arr - t_arr[0])) * 1000.0
+    return {"rate": lam, "requests": len(t_arr), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "solves_per_s": len(t_arr) / done.max(),
+            "all_converged": ok,
+            "path": "sp_rve_homogenize, FP64 ELL + FP64 Jacobi-PCG, one request at a time, "
+                    "7 load cases, cold start"}
+
+
+def serving(mb, args):
+    """Open-loop Poisson load on the device-resident server over 256 resident
+    geometries, in both warm-start modes, and the plain comparator replayed
+    on the first requests of the lowest-rate trace."""
+    geoms = serve_geometries(mb, args.serve_geoms, 4321)
+    traces = serve_traces(args, len(geoms))
+    out = {"geometries": len(geoms), "n_range": [8, 32], "budget_bytes": 150 * 10 ** 9}
+    out["warm_last"] = serve_mode(mb, geoms, traces, mb.SP_WARM_LAST)
+    out["warm_last"]["warm_start"] = ("each load case starts from the geometry's last solution "
+                                      "of it; every request is solved by CG to 1e-8")
+    out["predict"] = serve_mode(mb, geoms, traces, mb.SP_WARM_PREDICT)
+    out["predict"]["warm_start"] = ("first-order prediction from the geometry's last solved "
+                                    "request, verified by the FP64 residual; requests that miss "
+                                    "1e-8 are solved")
+    plain = plain_replay(mb, geoms, traces[0], args.plain_replay)
+    out["plain"] = plain
+    # capacity against the plain path: the saturated batched rate (highest
+    # arrival rate) over the plain path's rate under its own overload
+    top = str(traces[-1][0])
+    out["speedup_vs_plain"] = {
+        "warm_last": out["warm_last"]["rates"][top]["solves_per_s"] / plain["solves_per_s"],
+        "predict": out["predict"]["rates"][top]["solves_per_s"] / plain["solves_per_s"],
+        "at_rate": traces[-1][0]}
+    return out
+
+
+def ell_batch(mb, descs, args, stream, sptr, steps: int = 2):
+    """The same mix on the assembled operator (SP_OP_ELL): every launch
+    assembles each RVE's FP32 ELL values (8-colour scatter, node-sliced
+    copy) and runs the FP32 CG on them, FP64 refinement as in the headline.
+    One warm-up launch, then `steps` launches timed with CUDA events."""
+    import torch
+    t0 = time.time()
+    b = mb.Batch(descs, nrhs=6, inner_rtol=args.inner_rtol, op=mb.SP_OP_ELL)
+    setup = time.time() - t0
+    try:
+        b.launch(sptr)
+        torch.cuda.synchronize()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        evs[0].record(stream)
+        for k in range(steps):
+            b.launch(sptr)
+            evs[k + 1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(evs[k].elapsed_time(evs[k + 1]) for k in range(steps)) / steps
+        info = (mb.sp_solve_info * len(descs))()
+        b.download(None, None, info, sptr)
+        torch.cuda.synchronize()
+        inf = mb.info_array(info)
+        shape = b.shape()
+        return {"value": len(descs) / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms,
+                "steps": steps, "operator": "assembled FP32 ELL (node-sliced), assembly in the launch",
+                "cta_threads": shape[0], "ctas_per_sm": shape[1],
+                "converged": bool((inf["status"] == 0).all()),
+                "max_relres": float(inf["relres"].max()),
+                "mean_inner_its": float(inf["inner"].mean()),
+                "device_bytes": b.device_bytes(), "setup_s": setup}
+    finally:
+        b.close()
 
 
 def plain_gpu(mb, descs, args):
@@ -680,19 +811,25 @@ def main(argv=None):
     ap.add_argument("--sizes", type=int, nargs="+", default=list(SIZES),
                     help="mesh sizes to draw from (the headline workload uses 8 12 16 20)")
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--plain-per-size", type=int, default=2)
+    ap.add_argument("--plain-per-size", type=int, default=16)
+    ap.add_argument("--oracle-sample", type=int, default=8,
+                    help="RVEs per mesh size checked against the oracle after timing")
+    ap.add_argument("--no-ell", action="store_true",
+                    help="skip the assembled-ELL batched rate on the same mix")
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--no-fe2", action="store_true")
-    ap.add_argument("--fe2-per-gp", action="store_true",
-                    help="also time one Newton iteration with a serving request per Gauss point")
+    ap.add_argument("--no-fe2-per-gp", action="store_true",
+                    help="skip the FE2 run with a serving request per Gauss point")
     ap.add_argument("--serve-geoms", type=int, default=256)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[1e3, 1e4, 1e5])
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-max-req", type=int, default=4000)
+    ap.add_argument("--plain-replay", type=int, default=200,
+                    help="requests of the lowest-rate trace served by the plain path")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         run_reference(args)

@@ -72,10 +72,17 @@ int sp_ell_dev_free(sp_ell_dev *a);
 int sp_ell_dev_mvp(sp_ell_dev *a, const double *x_dev, double *y_dev, void *stream);
 /* Same with host vectors (copies in and out). */
 int sp_ell_dev_mvp_host(sp_ell_dev *a, const double *x, double *y);
-/* Lanes per row of sp_ell_dev_mvp: 4, 8, 16 or 32 (0: the library's choice,
- * 8 for 84-slot rows).  A tuning knob; the result does not depend on it
+/* Lanes per row of sp_ell_dev_mvp: 4, 8, 16 or 32 (0: the autotuner's
+ * choice).  For 84-slot (RVE-shaped) rows, sp_ell_upload times every width
+ * on the uploaded matrix and keeps the fastest (cached per device, row width
+ * and row-count octave).  A tuning knob; the result does not depend on it
  * beyond rounding. */
 int sp_ell_dev_set_lanes(sp_ell_dev *a, int lanes);
+/* The lanes per row sp_ell_dev_mvp uses, the upload-time trial's time per
+ * launch at 4, 8, 16 and 32 lanes (microseconds; trial_us may be NULL) and
+ * whether the choice came from the autotuner's cache.  No counterpart in the
+ * reference (its ell_mvp is a serial row loop, src/ell.c:127-141). */
+int sp_ell_dev_lanes(const sp_ell_dev *a, int *lanes, float *trial_us, int *from_cache);
 /* Rows, padded row width and stored (non-empty) slots of a device matrix. */
 int sp_ell_dev_info(const sp_ell_dev *a, int *nrow, int *wp, long long *true_nnz);
 /* Jacobi-preconditioned CG in FP64 on host vectors: the ELL path of the
@@ -199,14 +206,25 @@ typedef struct {
   double inner_rtol; /* CG residual reduction per refinement step (default 1e-4) */
   int max_outer;     /* refinement steps (default 8) */
   int max_inner;     /* CG iterations per step (default 4000) */
-  int threads;       /* threads per CTA (0: 512) */
-  int lanes_per_row; /* lanes per ELL row in the SpMM, 4..32 (0: tuned) */
+  int threads;       /* threads per CTA: 256, 512, 1024 (0: chosen, see tune) */
+  int lanes_per_row; /* unused by the batch: its operators give every lane one node */
   int ctas_per_sm;   /* resident CTAs per SM: 1 (1024 threads), 1 or 2 (512), 2 or 4 (256);
-                        0: 1 for the stencil, 2 for the assembled operator */
+                        0: chosen, see tune */
   int cluster;       /* CTAs (thread-block cluster) solving one RVE: 1, 2, 4, 8 (assembled) */
   int op;            /* SP_OP_STENCIL (default) or SP_OP_ELL */
   int bc;            /* SP_BC_AFFINE (default) or SP_BC_PERIODIC (stencil only) */
+  int tune;          /* with threads, ctas_per_sm 0 and cluster 1: SP_TUNE_AUTO (default)
+                        times every instantiated CTA shape (threads x CTAs per SM, i.e.
+                        registers per thread) on a sample of the batch at create time and
+                        keeps the fastest, cached per device, kernel, precision, load cases
+                        and dominant mesh size; SP_TUNE_OFF takes the fixed defaults (512 x 1
+                        for the stencil, 512 x 2 for the assembled operator).  A tuned
+                        batch's results do not depend on the launch, but the shape -- and so
+                        the last bits of the sums -- may depend on the batch's composition;
+                        fix threads and ctas_per_sm for bit-identical results across batches */
 } sp_batch_opts;
+#define SP_TUNE_AUTO 0
+#define SP_TUNE_OFF 1
 
 void sp_batch_opts_default(sp_batch_opts *o);
 
@@ -243,6 +261,16 @@ int sp_batch_homogenize(sp_batch *b, const double *strains, const double *materi
                         double *stress, double *strain, sp_solve_info *info, void *stream);
 /* The CTA shape and persistent grid the batch launches with. */
 int sp_batch_shape(const sp_batch *b, int *threads, int *ctas_per_sm, int *grid);
+/* The autotuner's trial of this batch's shape: up to `max` candidates with
+ * their threads, CTAs per SM and measured rate (estimated work units per ms:
+ * sum over the trial's RVEs of dof x mesh edge), the index of the chosen one,
+ * and whether the choice came from the process-wide cache (a batch of an
+ * earlier create with the same key).  *ntried = 0 when the caller fixed the
+ * shape.  No counterpart in the reference, which has no GPU kernels to tune;
+ * it stands in for run-time solver choice (KSPSetFromOptions,
+ * micro/src/alloc.c:42-43). */
+int sp_batch_tune_report(const sp_batch *b, int max, int *threads, int *ctas_per_sm,
+                         double *rate, int *ntried, int *chosen, int *from_cache);
 /* Kernel launches made by the last sp_batch_launch (for accounting). */
 int sp_batch_last_launches(const sp_batch *b, int *launches);
 
@@ -266,7 +294,13 @@ typedef struct {
   double refine_rtol;   /* a request whose warm-start prediction misses rtol is solved to
                            this tighter tolerance, so that predictions from its solutions
                            meet rtol without a solve (0: rtol / 100) */
+  int warm_start;       /* SP_WARM_PREDICT (default): first-order prediction from the
+                           geometry's last solved request; SP_WARM_LAST: each load case
+                           starts from the geometry's last solution of that load case, and
+                           every request is solved to rtol and kept as the next start */
 } sp_server_opts;
+#define SP_WARM_PREDICT 0
+#define SP_WARM_LAST 1
 
 void sp_server_opts_default(sp_server_opts *o);
 
@@ -289,6 +323,13 @@ int sp_server_submit(sp_server *s, int geometry, const double *strain, long long
  * stress[6], tangent[36] (row-major C[i][j] = d sigma_i / d eps_j). */
 int sp_server_poll(sp_server *s, long long ticket, double *stress, double *tangent,
                    sp_solve_info *info);
+/* Whether the loop is on the device now (it returns by itself after
+ * idle_spin_limit empty polls and is relaunched by the next submit or poll
+ * that finds work pending), how many times it has been launched, and how
+ * many requests were submitted.  No counterpart in the reference, whose
+ * request loop blocks in MPI_Recv (micro/src/main.c:114-120). */
+int sp_server_status(const sp_server *s, int *loop_on_device, long long *launches,
+                     long long *submitted);
 /* Stops the device loop after the queued requests finish. */
 int sp_server_stop(sp_server *s);
 /* Open-loop load generator on the calling host thread: request i (geometry

@@ -23,6 +23,7 @@ SP_ID_MATRIX, SP_ID_FIBER = 0, 1
 SP_PREC_MIXED, SP_PREC_FP64 = 0, 1
 SP_OP_ELL, SP_OP_STENCIL = 0, 1
 SP_BC_AFFINE, SP_BC_PERIODIC = 0, 1
+SP_TUNE_AUTO, SP_TUNE_OFF = 0, 1
 SP_MAX_RHS = 8
 SP_NOALLOC_MAX_ROWS = 262144
 MAX_ITS, MIN_ERR = 100000, 1.0e-10
@@ -66,19 +67,20 @@ class sp_batch_opts(C.Structure):
     _fields_ = [("nrhs", C.c_int), ("precision", C.c_int), ("rtol", C.c_double),
                 ("inner_rtol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
                 ("threads", C.c_int), ("lanes_per_row", C.c_int), ("ctas_per_sm", C.c_int),
-                ("cluster", C.c_int), ("op", C.c_int), ("bc", C.c_int)]
+                ("cluster", C.c_int), ("op", C.c_int), ("bc", C.c_int), ("tune", C.c_int)]
 
 
 class sp_server_opts(C.Structure):
     _fields_ = [("hbm_budget", C.c_size_t), ("max_inflight", C.c_int),
                 ("queue_capacity", C.c_int), ("rtol", C.c_double), ("inner_rtol", C.c_double),
                 ("idle_spin_limit", C.c_int), ("op", C.c_int), ("ctas_per_sm", C.c_int),
-                ("refine_rtol", C.c_double)]
+                ("refine_rtol", C.c_double), ("warm_start", C.c_int)]
 
 
 SP_ACTION_NULL, SP_ACTION_MICRO_CALC_STRESS, SP_ACTION_MICRO_CALC_C_TANGENT = 0, 1, 2
 SP_ACTION_MICRO_CALC_RHO, SP_ACTION_MICRO_END = 3, 4
 SP_MICRO_LINEAR, SP_MICRO_SOLVE = 0, 1
+SP_WARM_PREDICT, SP_WARM_LAST = 0, 1
 
 
 class sp_message(C.Structure):
@@ -182,6 +184,9 @@ _PROTOS = {
     "sp_batch_set_etype": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_ubyte), _vp]),
     "sp_batch_device_bytes": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "sp_batch_shape": (C.c_int, [_vp, _ip, _ip, _ip]),
+    "sp_batch_tune_report": (C.c_int, [_vp, C.c_int, _ip, _ip, _dp, _ip, _ip, _ip]),
+    "sp_ell_dev_lanes": (C.c_int, [_vp, _ip, C.POINTER(C.c_float), _ip]),
+    "sp_server_status": (C.c_int, [_vp, _ip, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "sp_batch_upload": (C.c_int, [_vp, _dp, _dp, _vp]),
     "sp_batch_launch": (C.c_int, [_vp, _vp]),
     "sp_batch_download": (C.c_int, [_vp, _dp, _dp, C.POINTER(sp_solve_info), _vp]),
@@ -421,6 +426,23 @@ class Batch:
         check(lib().sp_batch_shape(self.h, C.byref(t), C.byref(c), C.byref(g)), "sp_batch_shape")
         return t.value, c.value, g.value
 
+    def tune_report(self) -> dict:
+        """The autotuner's trial: candidate shapes with their measured rates
+        (estimated work units per ms), the chosen one, and whether it came
+        from the process-wide cache; empty when the shape was given."""
+        th = (C.c_int * 8)()
+        ct = (C.c_int * 8)()
+        rt = (C.c_double * 8)()
+        n, ch, fc = C.c_int(), C.c_int(), C.c_int()
+        check(lib().sp_batch_tune_report(self.h, 8, th, ct, rt, C.byref(n), C.byref(ch),
+                                         C.byref(fc)), "sp_batch_tune_report")
+        if n.value == 0:
+            return {}
+        return {"candidates": [{"threads": th[k], "ctas_per_sm": ct[k], "rate": rt[k]}
+                               for k in range(n.value)],
+                "chosen": {"threads": th[ch.value], "ctas_per_sm": ct[ch.value]},
+                "from_cache": bool(fc.value)}
+
     def device_bytes(self) -> int:
         b = C.c_size_t()
         check(lib().sp_batch_device_bytes(self.h, C.byref(b)), "sp_batch_device_bytes")
@@ -542,6 +564,13 @@ class Server:
         check(lib().sp_server_replay(self.h, n, ptr(g, _ip), ptr(s), ptr(ta), ptr(td), ptr(st),
                                      ptr(tg), info, timeout), "sp_server_replay")
         return td, st, tg.reshape(n, 6, 6), info
+
+    def status(self):
+        """(loop on the device now, launches of the loop so far, requests submitted)."""
+        on, n, sub = C.c_int(), C.c_longlong(), C.c_longlong()
+        check(lib().sp_server_status(self.h, C.byref(on), C.byref(n), C.byref(sub)),
+              "sp_server_status")
+        return bool(on.value), n.value, sub.value
 
     def stop(self):
         check(lib().sp_server_stop(self.h), "sp_server_stop")

@@ -9,6 +9,10 @@
 // are bit-identical to the reference's src/ell.c:127-184.
 #include <mutex>
 
+#include <algorithm>
+#include <array>
+#include <map>
+
 #include "ell.h"
 #include "pcg.cuh"
 #include "sp_cuda.h"
@@ -302,7 +306,10 @@ extern "C" int ell_solve_jacobi(ell_solver *solver, ell_matrix *m, double *b, do
 
 struct sp_ell_dev_s {
   int nrow, ncol, nnz, wp, dev;
-  int lanes = 0;  // lanes per row of the SpMV (0: chosen by the library)
+  int lanes = 0;  // lanes per row of the SpMV set by the caller (0: the tuned choice)
+  int lanes_tuned = 8;  // the autotuner's choice for this matrix
+  float trial_us[4] = {0.f, 0.f, 0.f, 0.f};  // trial time per launch at 4, 8, 16, 32 lanes
+  int tune_cached = 0;
   long long true_nnz = 0;  // stored (non-empty) slots
   int *cols = nullptr;    // [nrow][wp]
   double *vals = nullptr; // [nrow][wp]
@@ -313,6 +320,119 @@ struct sp_ell_dev_s {
   unsigned *ticket = nullptr;
   PcgGraph<double, 1, 32> *pcg = nullptr;
 };
+
+static void launch_spmv_rve(int L, int nb, cudaStream_t s, const sp_ell_dev_s *a, const double *x,
+                            double *y) {
+  switch (L) {
+    case 4: k_spmv_rve<4><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x, y); break;
+    case 8: k_spmv_rve<8><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x, y); break;
+    case 16: k_spmv_rve<16><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x, y); break;
+    default: k_spmv_rve<32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x, y); break;
+  }
+}
+
+// Reads a buffer larger than L2 (16-byte loads, one store only if the sum
+// is a value the buffer cannot hold), so that the next launch finds none of
+// its own data in L2 -- a read leaves clean lines, so no write-back lands in
+// the next launch.
+__global__ void k_l2_evict(const int4 *__restrict__ buf, size_t n16, int *sink) {
+  int acc = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int4 v = buf[i];
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  if (acc == 0x7fffffff) *sink = acc;  // never: the buffer is zero
+}
+
+// Lanes-per-row autotuner of the RVE-shaped SpMV: every instantiated width
+// (4, 8, 16, 32 lanes, i.e. 8, 4, 2, 1 rows per warp) is timed on the
+// uploaded matrix itself (one launch to load the kernel, then the best of 3
+// timed launches, x = 0 in the matrix's own scratch vectors), and the
+// fastest is kept.  A matrix larger than half the L2 streams from HBM in
+// use, so its trial launches start from an L2 emptied by reading a scratch
+// buffer of twice the L2 size (allocated for the trial only); a smaller
+// matrix is timed L2-warm, as it runs.  Choices are cached per device, row
+// width and row-count octave, so uploads of like matrices skip the trial.
+static std::mutex g_lanes_mu;
+static std::map<std::array<int, 3>, std::pair<int, std::array<float, 4>>> g_lanes_cache;
+
+static int tune_lanes(sp_ell_dev_s *a, Device *d) {
+  int oct = 0;
+  while ((1 << (oct + 1)) <= a->nrow) oct++;
+  const std::array<int, 3> key = {d->id, a->wp, oct};
+  {
+    std::lock_guard<std::mutex> lk(g_lanes_mu);
+    auto it = g_lanes_cache.find(key);
+    if (it != g_lanes_cache.end()) {
+      a->lanes_tuned = it->second.first;
+      for (int k = 0; k < 4; k++) a->trial_us[k] = it->second.second[k];
+      a->tune_cached = 1;
+      return SP_OK;
+    }
+  }
+  cudaStream_t s = d->stream;
+  double *x = a->vec, *y = a->vec + a->nrow;
+  cudaEvent_t e0, e1;
+  SP_CUDA_TRY(cudaMemsetAsync(x, 0, (size_t)a->nrow * sizeof(double), s));
+  int l2 = 0;
+  SP_CUDA_TRY(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, d->id));
+  const size_t mbytes = (size_t)a->nrow * a->wp * (sizeof(double) + sizeof(int));
+  int4 *flush = nullptr;
+  int *sink = nullptr;
+  const size_t fbytes = 2 * (size_t)l2;
+  if (mbytes > (size_t)l2 / 2) {
+    if (cudaMalloc((void **)&flush, fbytes + 16) != cudaSuccess) {
+      cudaGetLastError();
+      flush = nullptr;  // no room for the scratch: time L2-warm
+    } else {
+      sink = reinterpret_cast<int *>(reinterpret_cast<char *>(flush) + fbytes);
+      SP_CUDA_TRY(cudaMemsetAsync(flush, 0, fbytes, s));
+    }
+  }
+  SP_CUDA_TRY(cudaEventCreate(&e0));
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return sp_set_error(SP_ERR_CUDA, "sp_ell_upload: autotuner events");
+  }
+  const int widths[4] = {4, 8, 16, 32};
+  float best = 1e30f;
+  int rc = SP_OK;
+  for (int k = 0; k < 4 && !rc; k++) {
+    const int L = widths[k];
+    const int nb = launch_blocks(d, ((long long)a->nrow * L + 31) / 32);
+    launch_spmv_rve(L, nb, s, a, x, y);
+    float tmin = 1e30f;
+    for (int rep = 0; rep < 3 && !rc; rep++) {
+      float ms = 0.f;
+      if (flush) k_l2_evict<<<4 * d->nsm, 256, 0, s>>>(flush, fbytes / 16, sink);
+      cudaEventRecord(e0, s);
+      launch_spmv_rve(L, nb, s, a, x, y);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+        rc = sp_set_error(SP_ERR_CUDA, "sp_ell_upload: autotuner launch failed: %s",
+                          cudaGetErrorString(cudaGetLastError()));
+      tmin = std::min(tmin, ms);
+    }
+    a->trial_us[k] = 1000.f * tmin;
+    if (tmin < best) {
+      best = tmin;
+      a->lanes_tuned = L;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (flush) {
+    cudaStreamSynchronize(s);
+    cudaFree(flush);
+  }
+  if (!rc) {
+    std::lock_guard<std::mutex> lk(g_lanes_mu);
+    g_lanes_cache[key] = {a->lanes_tuned, {a->trial_us[0], a->trial_us[1], a->trial_us[2],
+                                           a->trial_us[3]}};
+  }
+  return rc;
+}
 
 extern "C" int sp_ell_upload(const ell_matrix *m, sp_ell_dev **out) {
   if (!m || !out || m->nrow <= 0 || m->nnz <= 0 || !m->cols || !m->vals)
@@ -364,6 +484,7 @@ extern "C" int sp_ell_upload(const ell_matrix *m, sp_ell_dev **out) {
   free(hc);
   free(hv);
   free(hd);
+  if (!rc && a->wp == SP_WP) rc = tune_lanes(a, d);
   if (rc) {
     sp_ell_dev_free(a);
     return rc;
@@ -392,15 +513,11 @@ extern "C" int sp_ell_dev_mvp(sp_ell_dev *a, const double *x_dev, double *y_dev,
   SP_TRY(device(&d));
   cudaStream_t s = pick_stream(stream, d);
   if (a->wp == SP_WP) {
-    // RVE-shaped rows: 84 slots, loads hoisted; 8 lanes (4 rows per warp) by default
-    const int L = a->lanes ? a->lanes : 8;
+    // RVE-shaped rows: 84 slots, loads hoisted; lanes per row from the
+    // caller or the upload-time autotuner
+    const int L = a->lanes ? a->lanes : a->lanes_tuned;
     int nb = launch_blocks(d, ((long long)a->nrow * L + 31) / 32);
-    switch (L) {
-      case 4: k_spmv_rve<4><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
-      case 8: k_spmv_rve<8><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
-      case 16: k_spmv_rve<16><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
-      default: k_spmv_rve<32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->vals, a->cols, x_dev, y_dev); break;
-    }
+    launch_spmv_rve(L, nb, s, a, x_dev, y_dev);
   } else {
     int nb = launch_blocks(d, a->nrow);
     k_spmm_plain<double, 1, 32><<<nb, PCG_THREADS, 0, s>>>(a->nrow, a->wp, a->vals, a->cols,
@@ -415,6 +532,15 @@ extern "C" int sp_ell_dev_set_lanes(sp_ell_dev *a, int lanes) {
   if (lanes != 0 && lanes != 4 && lanes != 8 && lanes != 16 && lanes != 32)
     return sp_set_error(SP_ERR_ARG, "sp_ell_dev_set_lanes: lanes must be 0, 4, 8, 16 or 32");
   a->lanes = lanes;
+  return SP_OK;
+}
+
+extern "C" int sp_ell_dev_lanes(const sp_ell_dev *a, int *lanes, float *trial_us, int *from_cache) {
+  if (!a) return sp_set_error(SP_ERR_ARG, "sp_ell_dev_lanes: null matrix");
+  if (lanes) *lanes = a->lanes ? a->lanes : a->lanes_tuned;
+  if (trial_us)
+    for (int k = 0; k < 4; k++) trial_us[k] = a->trial_us[k];
+  if (from_cache) *from_cache = a->tune_cached;
   return SP_OK;
 }
 

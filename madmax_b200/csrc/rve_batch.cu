@@ -25,7 +25,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "rve_batch_kernel.cuh"
@@ -43,6 +45,13 @@ SP_BATCH_SHAPES_FP64(SP_BATCH_EXTERN, double, 8)
 
 struct Shape {
   int threads, ctas, cluster, op;
+};
+
+constexpr int SP_TUNE_MAX = 8;
+struct TuneRecord {
+  int n = 0, best = 0, cached = 0;
+  Shape shape[SP_TUNE_MAX];
+  double rate[SP_TUNE_MAX];
 };
 
 template <typename T, int K>
@@ -77,6 +86,111 @@ static int kernel_op(const sp_batch_opts &o) {
   return (o.op == SP_OP_STENCIL && o.bc == SP_BC_PERIODIC) ? SP_OP_STENCIL_PER : o.op;
 }
 
+// A CTA shape's kernel, dynamic shared memory and persistent grid (as many
+// clusters as can be resident at once); returns an error for a shape that is
+// not instantiated or cannot be resident.
+static int shape_setup(const sp_batch_opts &o, int kp, const Device *d, const Shape &sh,
+                       BatchFn *fn_out, int *dyn_out, int *grid_out) {
+  BatchFn fn = pick(o.precision, kp, sh);
+  if (!fn)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: no kernel for %d threads x %d CTAs/SM, "
+                        "cluster %d, %s operator in this precision", sh.threads, sh.ctas,
+                        sh.cluster, o.op == SP_OP_ELL ? "assembled" : "stencil");
+  int g = d->nsm * sh.ctas;
+  const int dyn = sp_batch_uses_ptable(o.precision == SP_PREC_MIXED, kp, sh.op,
+                                       sh.threads * sh.ctas <= 512)
+                      ? SP_PT_BYTES
+                      : 0;
+  if (dyn && cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  dyn) != cudaSuccess) {
+    cudaGetLastError();
+    return sp_set_error(SP_ERR_CUDA, "sp_batch_create: %d bytes of dynamic shared memory refused",
+                        dyn);
+  }
+  if (sh.cluster == 1) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)fn, sh.threads, dyn) !=
+            cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      return sp_set_error(SP_ERR_CUDA, "sp_batch_create: %d-thread CTAs cannot be resident",
+                          sh.threads);
+    }
+    g = d->nsm * std::min(sh.ctas, nb);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g);
+    cfg.blockDim = dim3(sh.threads);
+    cfg.dynamicSmemBytes = dyn;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = sh.cluster;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, (void *)fn, &cfg) != cudaSuccess || ncl < 1) {
+      cudaGetLastError();
+      return sp_set_error(SP_ERR_CUDA, "sp_batch_create: cluster of %d CTAs cannot be resident",
+                          sh.cluster);
+    }
+    g = std::min(g, ncl * sh.cluster);
+  }
+  *fn_out = fn;
+  *dyn_out = dyn;
+  *grid_out = g;
+  return SP_OK;
+}
+
+static int launch_shape(BatchFn fn, const Shape &sh, int grid, int dyn, cudaStream_t s,
+                        const BatchParams &P) {
+  if (sh.cluster == 1) {
+    fn<<<grid, sh.threads, dyn, s>>>(P);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(sh.threads);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = sh.cluster;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    SP_CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, P));
+  }
+  SP_CUDA_TRY(cudaGetLastError());
+  return SP_OK;
+}
+
+// ------------------------------------------------------------ autotuner ---
+//
+// The instantiated one-CTA-per-RVE shapes of a kernel variant: threads per
+// CTA x CTAs per SM, which fixes the registers a thread may use (65,536 /
+// (threads x CTAs)): 128 at 512 x 1, 64 at 512 x 2 / 256 x 4 / 1024 x 1.
+static std::vector<Shape> tune_candidates(const sp_batch_opts &o) {
+  const int kop = kernel_op(o);
+  if (kop == SP_OP_STENCIL_PER || o.precision == SP_PREC_FP64)
+    return {{512, 1, 1, kop}, {512, 2, 1, kop}};
+  if (kop == SP_OP_STENCIL)
+    return {{512, 1, 1, kop}, {512, 2, 1, kop}, {256, 2, 1, kop}, {256, 4, 1, kop},
+            {1024, 1, 1, kop}};
+  return {{512, 1, 1, kop}, {512, 2, 1, kop}, {256, 2, 1, kop}, {256, 4, 1, kop}};
+}
+
+using TuneKey = std::array<int, 5>;  // device, kernel operator, precision, load cases, size class
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneRecord> g_tune_cache;
+
+// estimated cost of one RVE solve: dof x largest mesh edge (CG iterations
+// grow with the edge)
+static double rve_work(const MeshGeo &g) {
+  return (double)g.ndof * std::max(g.nex, std::max(g.ney, g.nez));
+}
+
 }  // namespace sp
 
 using namespace sp;
@@ -100,7 +214,85 @@ struct sp_batch_s {
   double *d_ws_u = nullptr;
   void *d_ws_v = nullptr, *d_ws_rm = nullptr, *d_ws_drm = nullptr, *d_ws_dinv = nullptr;
   size_t bytes = 0;
+  TuneRecord tune;  // the autotuner's trial (tune.n == 0: shape fixed by the caller)
+  int tune_slots = 0;  // work spaces allocated while the autotuner runs
 };
+
+// Time every candidate shape on the same sample of the batch: 2 G RVEs, G
+// the largest candidate grid, taken at even steps through the largest-first
+// order (the batch's size mix, in its order), after an empty launch that
+// loads the kernel.  The rate is the sample's estimated work over the
+// launch time.  (A sample of 2 grids per candidate gives every candidate
+// two waves, while the whole batch gives a small grid many more: the tail
+// of the last wave then weighs on a large grid's trial less than on its
+// real launches.)  The trial writes the outputs of the RVEs it solves; the
+// batch's own launches overwrite them.
+static int tune_trial(sp_batch *b, const std::vector<Shape> &cands, const std::vector<int> &order,
+                      const std::vector<double> &work, const Device *d, TuneRecord *rec) {
+  cudaStream_t s = d->stream;
+  const int nrve = b->nrve;
+  int *d_trial = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = SP_OK;
+  if (cudaMalloc((void **)&d_trial, (size_t)nrve * sizeof(int)) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: autotuner set-up failed");
+  }
+  rec->n = 0;
+  double best = -1.0;
+  // the common sample: 2 x the largest candidate grid (the work spaces hold
+  // that many slots)
+  const int T = std::min(nrve, 2 * b->tune_slots);
+  std::vector<int> sample(T);
+  double wsum = 0.0;
+  for (int j = 0; j < T; j++) {
+    sample[j] = order[(size_t)j * nrve / T];
+    wsum += work[sample[j]];
+  }
+  if (!rc && cudaMemcpyAsync(d_trial, sample.data(), T * sizeof(int), cudaMemcpyHostToDevice, s))
+    rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: autotuner upload failed");
+  for (size_t c = 0; c < cands.size() && !rc && rec->n < SP_TUNE_MAX; c++) {
+    BatchFn fn;
+    int dyn, grid;
+    if (shape_setup(b->o, b->kp, d, cands[c], &fn, &dyn, &grid) != SP_OK) continue;  // not resident
+    if (grid / cands[c].cluster > b->tune_slots) continue;  // work spaces sized for fewer
+    BatchParams P = b->P;
+    P.order = d_trial;
+    if (cudaMemsetAsync(b->d_counter, 0, sizeof(int), s)) {
+      rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: autotuner upload failed");
+      break;
+    }
+    P.nrve = 0;  // loads the kernel; every CTA finds no work
+    rc = launch_shape(fn, cands[c], grid, dyn, s, P);
+    if (rc) break;
+    P.nrve = T;
+    if (cudaMemsetAsync(b->d_counter, 0, sizeof(int), s) || cudaEventRecord(e0, s)) {
+      rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: autotuner launch failed");
+      break;
+    }
+    rc = launch_shape(fn, cands[c], grid, dyn, s, P);
+    if (rc) break;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, s) || cudaEventSynchronize(e1) || cudaEventElapsedTime(&ms, e0, e1)) {
+      rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: autotuner timing failed");
+      break;
+    }
+    const int k = rec->n++;
+    rec->shape[k] = cands[c];
+    rec->rate[k] = wsum / std::max(ms, 1e-3f);
+    if (rec->rate[k] > best) {
+      best = rec->rate[k];
+      rec->best = k;
+    }
+  }
+  if (!rc && rec->n == 0) rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: no CTA shape can run");
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(d_trial);
+  return rc;
+}
+
 
 extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   memset(o, 0, sizeof(*o));
@@ -147,6 +339,10 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   // 20-26% faster on n = 8-12; 2.3x faster than 512 x 2 under periodic
   // conditions, whose 64-register build spills), 512 x 2 for the assembled
   // operator.
+  if (o.tune != SP_TUNE_AUTO && o.tune != SP_TUNE_OFF)
+    return sp_set_error(SP_ERR_ARG, "sp_batch_create: tune must be SP_TUNE_AUTO or SP_TUNE_OFF");
+  // the autotuner picks the shape when the caller leaves it open
+  const bool tune = o.threads == 0 && o.ctas_per_sm == 0 && o.cluster <= 1 && o.tune == SP_TUNE_AUTO;
   const bool one = o.op == SP_OP_STENCIL && o.cluster <= 1;
   if (o.threads == 0) o.threads = 512;
   if (o.ctas_per_sm == 0) o.ctas_per_sm = (o.threads == 1024 || (one && o.threads == 512)) ? 1 : 2;
@@ -245,59 +441,58 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     return hplans[hrves[a].plan].geo.ndof > hplans[hrves[c].plan].geo.ndof;
   });
   int nrhs = o.nrhs, kp = b->kp;
-  // persistent grid: as many clusters as can be resident at once
-  {
+  // persistent grid: as many clusters as can be resident at once.  Left to
+  // the autotuner, the shape comes from the cache, or from a trial below
+  // once the batch's data are on the device (its work spaces sized for the
+  // largest candidate grid until then).
+  std::vector<Shape> cands;
+  std::vector<double> work(nrve);
+  TuneKey tkey = {};
+  bool trial = false;
+  if (tune && !rc) {
+    std::map<int, double> by_edge;
+    for (int i = 0; i < nrve; i++) {
+      const MeshGeo &g = hplans[hrves[i].plan].geo;
+      work[i] = rve_work(g);
+      by_edge[std::max(g.nex, std::max(g.ney, g.nez))] += work[i];
+    }
+    int dom = 0;
+    double wmax = -1.0;
+    for (auto &kv : by_edge)
+      if (kv.second > wmax) {
+        wmax = kv.second;
+        dom = kv.first;
+      }
+    tkey = {d->id, kernel_op(o), o.precision, kp, dom};
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(tkey);
+      if (it != g_tune_cache.end()) {
+        b->tune = it->second;
+        b->tune.cached = 1;
+      }
+    }
+    if (b->tune.n) {
+      const Shape &w = b->tune.shape[b->tune.best];
+      o.threads = w.threads;
+      o.ctas_per_sm = w.ctas;
+    } else {
+      trial = true;
+      cands = tune_candidates(o);
+      for (const Shape &c : cands) {
+        BatchFn fn;
+        int dyn, grid;
+        if (shape_setup(o, kp, d, c, &fn, &dyn, &grid) == SP_OK)
+          b->tune_slots = std::max(b->tune_slots, grid / c.cluster);
+      }
+      cudaGetLastError();
+    }
+    b->o = o;
+  }
+  if (!rc) {
     Shape sh{o.threads, o.ctas_per_sm, o.cluster, kernel_op(o)};
-    BatchFn fn = pick(o.precision, kp, sh);
-    if (!fn && !rc)
-      rc = sp_set_error(SP_ERR_ARG, "sp_batch_create: no kernel for %d threads x %d CTAs/SM, "
-                        "cluster %d, %s operator in this precision", o.threads, o.ctas_per_sm,
-                        o.cluster, o.op == SP_OP_ELL ? "assembled" : "stencil");
-    int g = d->nsm * o.ctas_per_sm;
-    b->dyn_smem = sp_batch_uses_ptable(o.precision == SP_PREC_MIXED, kp, kernel_op(o),
-                                       o.threads * o.ctas_per_sm <= 512)
-                      ? SP_PT_BYTES
-                      : 0;
-    if (fn && !rc && b->dyn_smem) {
-      if (cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               b->dyn_smem) != cudaSuccess) {
-        cudaGetLastError();
-        rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: %d bytes of dynamic shared memory refused",
-                          b->dyn_smem);
-      }
-    }
-    if (o.cluster == 1 && fn && !rc) {
-      int nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, (const void *)fn, o.threads,
-                                                        b->dyn_smem) != cudaSuccess || nb < 1) {
-        cudaGetLastError();
-        rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: %d-thread CTAs cannot be resident",
-                          o.threads);
-      } else {
-        g = d->nsm * std::min(o.ctas_per_sm, nb);
-      }
-    }
-    if (o.cluster > 1 && !rc) {
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(g);
-      cfg.blockDim = dim3(o.threads);
-      cfg.dynamicSmemBytes = b->dyn_smem;
-      cudaLaunchAttribute at;
-      at.id = cudaLaunchAttributeClusterDimension;
-      at.val.clusterDim.x = o.cluster;
-      at.val.clusterDim.y = 1;
-      at.val.clusterDim.z = 1;
-      cfg.attrs = &at;
-      cfg.numAttrs = 1;
-      int ncl = 0;
-      if (cudaOccupancyMaxActiveClusters(&ncl, (void *)fn, &cfg) != cudaSuccess || ncl < 1) {
-        cudaGetLastError();
-        rc = sp_set_error(SP_ERR_CUDA, "sp_batch_create: cluster of %d CTAs cannot be resident",
-                          o.cluster);
-      }
-      g = std::min(g, ncl * o.cluster);
-    }
-    b->grid = g;
+    BatchFn fn;
+    rc = shape_setup(o, kp, d, sh, &fn, &b->dyn_smem, &b->grid);
   }
   size_t stride = (size_t)kp * 3 * maxnp;
   // (3*maxnp >= maxdof; a multiple of 96, so every slot starts 16-byte aligned)
@@ -316,7 +511,8 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (!rc) rc = dmalloc((void **)&b->d_stress, (size_t)nrve * nrhs * 6 * sizeof(double), acct);
   if (!rc) rc = dmalloc((void **)&b->d_strain, (size_t)nrve * nrhs * 6 * sizeof(double), acct);
   if (!rc) rc = dmalloc((void **)&b->d_info, (size_t)nrve * sizeof(sp_solve_info), acct);
-  const size_t slots = (size_t)(b->grid / o.cluster);  // one work space per cluster
+  // one work space per cluster (for the largest candidate grid while tuning)
+  const size_t slots = (size_t)std::max(b->grid / o.cluster, b->tune_slots);
   if (!rc) rc = dmalloc((void **)&b->d_ws_u, slots * stride * sizeof(double), acct);
   if (!rc) rc = dmalloc(&b->d_ws_v, slots * 4 * stride * tsz, acct);
   if (!rc && ell) rc = dmalloc(&b->d_ws_rm, slots * rm_stride * tsz, acct);
@@ -374,6 +570,48 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   P.inner_rtol = o.inner_rtol;
   P.max_outer = o.max_outer;
   P.max_inner = o.max_inner;
+  if (trial) {
+    rc = tune_trial(b, cands, order, work, d, &b->tune);
+    if (!rc) {
+      const Shape &w = b->tune.shape[b->tune.best];
+      b->o.threads = w.threads;
+      b->o.ctas_per_sm = w.ctas;
+      BatchFn fn;
+      rc = shape_setup(b->o, kp, d, w, &fn, &b->dyn_smem, &b->grid);
+    }
+    if (!rc) {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune_cache[tkey] = b->tune;
+    }
+    // keep only the work spaces the chosen grid uses
+    const size_t keep = (size_t)(b->grid / b->o.cluster);
+    if (!rc && keep < slots) {
+      cudaFree(b->d_ws_u);
+      cudaFree(b->d_ws_v);
+      cudaFree(b->d_ws_rm);
+      cudaFree(b->d_ws_drm);
+      cudaFree(b->d_ws_dinv);
+      b->d_ws_u = nullptr;
+      b->d_ws_v = b->d_ws_rm = b->d_ws_drm = b->d_ws_dinv = nullptr;
+      b->bytes -= slots * (stride * sizeof(double) + 4 * stride * tsz +
+                           (ell ? rm_stride * tsz + drm_stride * tsz : drm_stride * tsz));
+      if (!rc) rc = dmalloc((void **)&b->d_ws_u, keep * stride * sizeof(double), acct);
+      if (!rc) rc = dmalloc(&b->d_ws_v, keep * 4 * stride * tsz, acct);
+      if (!rc && ell) rc = dmalloc(&b->d_ws_rm, keep * rm_stride * tsz, acct);
+      if (!rc && ell) rc = dmalloc(&b->d_ws_drm, keep * drm_stride * tsz, acct);
+      if (!rc && !ell) rc = dmalloc(&b->d_ws_dinv, keep * drm_stride * tsz, acct);
+      P.ws_u = b->d_ws_u;
+      P.ws_v = b->d_ws_v;
+      P.ws_rm = b->d_ws_rm;
+      P.ws_drm = b->d_ws_drm;
+      P.ws_dinv = b->d_ws_dinv;
+    }
+    b->tune_slots = 0;
+    if (rc) {
+      sp_batch_destroy(b);
+      return rc;
+    }
+  }
   *out = b;
   return SP_OK;
 }
@@ -427,24 +665,7 @@ extern "C" int sp_batch_launch(sp_batch *b, void *stream) {
   Shape sh{b->o.threads, b->o.ctas_per_sm, b->o.cluster, kernel_op(b->o)};
   BatchFn fn = pick(b->o.precision, b->nrhs, sh);
   SP_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
-  if (b->o.cluster == 1) {
-    fn<<<b->grid, b->o.threads, b->dyn_smem, s>>>(b->P);
-  } else {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(b->grid);
-    cfg.blockDim = dim3(b->o.threads);
-    cfg.dynamicSmemBytes = b->dyn_smem;
-    cfg.stream = s;
-    cudaLaunchAttribute at;
-    at.id = cudaLaunchAttributeClusterDimension;
-    at.val.clusterDim.x = b->o.cluster;
-    at.val.clusterDim.y = 1;
-    at.val.clusterDim.z = 1;
-    cfg.attrs = &at;
-    cfg.numAttrs = 1;
-    SP_CUDA_TRY(cudaLaunchKernelEx(&cfg, fn, b->P));
-  }
-  SP_CUDA_TRY(cudaGetLastError());
+  SP_TRY(launch_shape(fn, sh, b->grid, b->dyn_smem, s, b->P));
   b->last_launches = 1;
   return SP_OK;
 }
@@ -478,6 +699,21 @@ extern "C" int sp_batch_homogenize(sp_batch *b, const double *strains, const dou
   if (info)
     for (int i = 0; i < b->nrve; i++)
       if (info[i].status) return sp_set_error(SP_ERR_NOCONV, "RVE %d did not converge (relres %.3e)", i, info[i].relres);
+  return SP_OK;
+}
+
+extern "C" int sp_batch_tune_report(const sp_batch *b, int max, int *threads, int *ctas_per_sm,
+                                    double *rate, int *ntried, int *chosen, int *from_cache) {
+  if (!b) return sp_set_error(SP_ERR_ARG, "null batch");
+  const TuneRecord &r = b->tune;
+  for (int k = 0; k < r.n && k < max; k++) {
+    if (threads) threads[k] = r.shape[k].threads;
+    if (ctas_per_sm) ctas_per_sm[k] = r.shape[k].ctas;
+    if (rate) rate[k] = r.rate[k];
+  }
+  if (ntried) *ntried = r.n;
+  if (chosen) *chosen = r.best;
+  if (from_cache) *from_cache = r.cached;
   return SP_OK;
 }
 

@@ -986,6 +986,24 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
   }
 }
 
+// The pattern-table block of a node with material mask `mask` (bit c: the
+// element at corner c) for the neighbour at offset (dx, dy, dz).
+__device__ __forceinline__ int sp_pt_index(unsigned mask, int dx, int dy, int dz) {
+  unsigned q0 = 0, q1 = 0;
+  int nb = 0;
+#pragma unroll
+  for (int c2 = 0; c2 < 4; c2++) {
+    const int ox = c2 & 1, oy = c2 >> 1;
+    if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
+    q0 |= ((mask >> c2) & 1u) << nb;
+    q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
+    nb++;
+  }
+  const int m0 = (dx + 1) + 3 * (dy + 1);
+  return dz < 0 ? sp_pt_off(m0) + (int)q0
+                : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb)) : sp_pt_off(m0 + 18) + (int)q1);
+}
+
 // FP32 stencil SpMM under Dirichlet conditions with the x-neighbours taken
 // from the warp.  A warp holds 32 consecutive interior nodes: lanes 1..30
 // produce output, lanes 0 and 31 only supply values.  For each of the 9
@@ -1032,9 +1050,132 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
     for (int d = 0; d < 3; d++)
 #pragma unroll
       for (int p = 0; p < KP; p++) acc[d][p] = make_float2(0.f, 0.f);
+    // the 9 (dy, dz) rows in turn, the next row's gathers issued before the
+    // current row's products (two row buffers in registers)
+    float2 xr[2][3][KP];
+    auto gather = [&](int r, float2 (&xv)[3][KP]) {
+      const int dy = r % 3 - 1, dz = r / 3 - 1;
+      const float *xb = x + nbk_base<K>(a + dy * sy + dz * sz);
+#pragma unroll
+      for (int p = 0; p < KP; p++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          xv[c][p] = make_float2(0.f, 0.f);
+          if ((amask >> (2 * p)) & 3u) {
+            xv[c][p].x = xb[(c * K + 2 * p) * 32];
+            if (2 * p + 1 < K) xv[c][p].y = xb[(c * K + 2 * p + 1) * 32];
+          }
+        }
+    };
+    gather(0, xr[0]);
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+      const int dy = r % 3 - 1, dz = r / 3 - 1;
+      if (r + 1 < 9) gather(r + 1, xr[(r + 1) & 1]);
+      const float2 (&xv)[3][KP] = xr[r & 1];
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++) {
+        float bv[9] = {};
+        add_block<float, float>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
+#pragma unroll
+        for (int p = 0; p < KP; p++) {
+          if (!((amask >> (2 * p)) & 3u)) continue;
+          float2 xs[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) {
+            if (dx == 0) {
+              xs[c] = xv[c][p];
+            } else {
+              float2 v;
+              if (dx < 0) {
+                v.x = __shfl_up_sync(FULL, xv[c][p].x, 1);
+                v.y = __shfl_up_sync(FULL, xv[c][p].y, 1);
+              } else {
+                v.x = __shfl_down_sync(FULL, xv[c][p].x, 1);
+                v.y = __shfl_down_sync(FULL, xv[c][p].y, 1);
+              }
+              xs[c] = (dx < 0 ? lo : hi) ? v : make_float2(0.f, 0.f);
+            }
+          }
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const float b = bv[d * 3 + c];
+              acc[d][p] = __ffma2_rn(make_float2(b, b), xs[c], acc[d][p]);
+            }
+        }
+      }
+    }
+    if (out) {
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        if (!((amask >> q) & 1u)) continue;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const float yv = (q & 1) ? acc[d][q >> 1].y : acc[d][q >> 1].x;
+          dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
+          y[q * blk + (size_t)d * g.nn_pad + a] = yv;
+        }
+      }
+    }
+  }
+}
+
+// The FP32 Dirichlet stencil SpMM of spmm_stencil_xw with the x-neighbour
+// exchange moved from the inputs to the outputs.  The operator is
+// symmetric, so the dx = -1 term of node i+1, B_{i+1}(-1, dy, dz) x_{i +
+// (0, dy, dz)}, multiplies the value lane i gathered for its own column: lane
+// i forms it with lane i+1's block (pattern from lane i+1's material mask)
+// and likewise the dx = +1 term of node i-1.  The three sums are kept apart
+// over all 9 (dy, dz) rows and the neighbours' parts cross lanes once per
+// warp trip (2 x 3K shuffles instead of 2 x 3K per row); a lane adds the
+// part from lane i-1 (i+1) only when that lane holds its x-neighbour, i.e.
+// unless its node is first (last) in its x-row of interior nodes.
+template <int K>
+__device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const float *KB,
+                                       const uint8_t *__restrict__ etype, const float *x,
+                                       float *y, double *dot, unsigned amask, bool rev) {
+  constexpr int KP = (K + 1) / 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
+  const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
+  const int ni = mx * my * mz;
+  const int sy = g.nx, sz = g.nx * g.ny;
+  const int esy = g.nex, esz = g.nex * g.ney;
+  const size_t blk = (size_t)3 * g.nn_pad;
+  const int ngr = (ni + 29) / 30;
+  for (int gi = warp; gi < ngr; gi += nwarps) {
+    const int s0 = (rev ? ngr - 1 - gi : gi) * 30;
+    const int id = s0 - 1 + lane;
+    const bool out = lane >= 1 && lane <= 30 && id < ni;
+    const int idc = min(max(id, 0), ni - 1);
+    const int ii = idc % mx, jj = (idc / mx) % my, kk = idc / (mx * my);
+    const int i = ii + 1, j = jj + 1, k = kk + 1;
+    const int a = i + j * sy + k * sz;
+    const bool lo = ii > 0, hi = ii < mx - 1;
+    unsigned mask = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+      const int e = (i - 1 + ox) + (j - 1 + oy) * esy + (k - 1 + oz) * esz;
+      mask |= (unsigned)__ldg(etype + e) << c;
+    }
+    const unsigned mr = __shfl_down_sync(FULL, mask, 1);  // lane i+1's materials
+    const unsigned ml = __shfl_up_sync(FULL, mask, 1);    // lane i-1's materials
+    float2 acc[3][KP], accr[3][KP], accl[3][KP];
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int p = 0; p < KP; p++)
+        acc[d][p] = accr[d][p] = accl[d][p] = make_float2(0.f, 0.f);
 #pragma unroll 1
     for (int dz = -1; dz <= 1; dz++) {
+#if defined(SP_XO_ROW1)
+#pragma unroll 1
+#else
 #pragma unroll
+#endif
       for (int dy = -1; dy <= 1; dy++) {
         const float *xb = x + nbk_base<K>(a + dy * sy + dz * sz);
         float2 xv[3][KP];
@@ -1048,57 +1189,48 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
               if (2 * p + 1 < K) xv[c][p].y = xb[(c * K + 2 * p + 1) * 32];
             }
           }
+        // own block (dx = 0), lane i+1's dx = -1 block, lane i-1's dx = +1 block
 #pragma unroll
-        for (int dx = -1; dx <= 1; dx++) {
-          // pattern bits of the shared elements: layer oz = 0 (q0) and oz = 1
-          // (q1) of the (ox, oy) corners that the x and y offsets allow
-          unsigned q0 = 0, q1 = 0;
-          int nb = 0;
-#pragma unroll
-          for (int c2 = 0; c2 < 4; c2++) {
-            const int ox = c2 & 1, oy = c2 >> 1;
-            if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
-            q0 |= ((mask >> c2) & 1u) << nb;
-            q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
-            nb++;
-          }
-          const int m0 = (dx + 1) + 3 * (dy + 1);
-          const int idx = dz < 0 ? sp_pt_off(m0) + (int)q0
-                                 : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb))
-                                            : sp_pt_off(m0 + 18) + (int)q1);
+        for (int w = 0; w < 3; w++) {
+          const int idx = w == 0 ? sp_pt_index(mask, 0, dy, dz)
+                                 : (w == 1 ? sp_pt_index(mr, -1, dy, dz) : sp_pt_index(ml, 1, dy, dz));
           float bv[9] = {};
           add_block<float, float>(KB + idx * SP_PT_REC, bv);
+          float2 (&ac)[3][KP] = w == 0 ? acc : (w == 1 ? accr : accl);
 #pragma unroll
           for (int p = 0; p < KP; p++) {
             if (!((amask >> (2 * p)) & 3u)) continue;
-            float2 xs[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-              if (dx == 0) {
-                xs[c] = xv[c][p];
-              } else {
-                float2 v;
-                if (dx < 0) {
-                  v.x = __shfl_up_sync(FULL, xv[c][p].x, 1);
-                  v.y = __shfl_up_sync(FULL, xv[c][p].y, 1);
-                } else {
-                  v.x = __shfl_down_sync(FULL, xv[c][p].x, 1);
-                  v.y = __shfl_down_sync(FULL, xv[c][p].y, 1);
-                }
-                xs[c] = (dx < 0 ? lo : hi) ? v : make_float2(0.f, 0.f);
-              }
-            }
 #pragma unroll
             for (int d = 0; d < 3; d++)
 #pragma unroll
               for (int c = 0; c < 3; c++) {
                 const float b = bv[d * 3 + c];
-                acc[d][p] = __ffma2_rn(make_float2(b, b), xs[c], acc[d][p]);
+                ac[d][p] = __ffma2_rn(make_float2(b, b), xv[c][p], ac[d][p]);
               }
           }
         }
       }
     }
+    // the neighbours' parts: lane i-1's accr and lane i+1's accl
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int p = 0; p < KP; p++) {
+        if (!((amask >> (2 * p)) & 3u)) continue;
+        float2 fl, fr;
+        fl.x = __shfl_up_sync(FULL, accr[d][p].x, 1);
+        fl.y = __shfl_up_sync(FULL, accr[d][p].y, 1);
+        fr.x = __shfl_down_sync(FULL, accl[d][p].x, 1);
+        fr.y = __shfl_down_sync(FULL, accl[d][p].y, 1);
+        if (lo) {
+          acc[d][p].x += fl.x;
+          acc[d][p].y += fl.y;
+        }
+        if (hi) {
+          acc[d][p].x += fr.x;
+          acc[d][p].y += fr.y;
+        }
+      }
     if (out) {
 #pragma unroll
       for (int q = 0; q < K; q++) {

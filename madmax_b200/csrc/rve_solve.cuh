@@ -142,7 +142,11 @@ struct StencilOp {
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
                         unsigned amask, bool rev) const {
     if constexpr (PT)
+#if defined(SP_XO)
+      spmm_stencil_xo<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+#else
       spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+#endif
     else
       spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
   }

@@ -19,7 +19,9 @@
 //     geometry's previous solution, writes the result to mapped memory and
 //     raises the request's done flag.  The warm start is a first-order
 //     prediction from the previous request's 7 solutions (u(eps) and
-//     u(eps + delta e_i) give the derivative of u in every strain direction).
+//     u(eps + delta e_i) give the derivative of u in every strain direction),
+//     or (SP_WARM_LAST) the previous request's solution of each load case
+//     as it is.
 // A request is picked up as soon as any slot is free, while other requests
 // are still solving: their work overlaps on the device.  Every wait is
 // bounded (idle_spin_limit polls); on expiry the CTA returns and the host
@@ -101,6 +103,7 @@ struct ServeParams {
   size_t stride;
   double rtol, inner_rtol, refine_rtol;
   int max_outer, max_inner, idle_limit;
+  int warm_last;  // SP_WARM_LAST: start from the last solutions, no prediction
 };
 
 // Prepare every geometry once (a CTA takes geometries in turn): element
@@ -339,7 +342,10 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
         for (int c = 0; c < 6; c++) s += seps[t * 6 + a] * __ldg(G.gram + a * 6 + c) * seps[t * 6 + c];
       srn0[t] = sqrt(fmax(s, 0.0));
     }
-    if (warm) {
+    if (warm && P.warm_last) {
+      // the last request's solution of each load case, as it is
+      for (size_t i = t; i < nu; i += SERVE_NT) u[i] = __ldcg(G.warm + i);
+    } else if (warm) {
       if (t < SERVE_K * 6) {
         const int k = t / 6, j = t % 6;
         const double e0 = __ldcg(G.warm_eps + j);
@@ -374,8 +380,9 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     sa.nrhs = SERVE_NRHS;
     sa.rtol = P.rtol;
     // a request whose prediction misses rtol is solved tighter, so that the
-    // predictions from its solutions meet rtol without a solve
-    sa.rtol_refine = P.refine_rtol;
+    // predictions from its solutions meet rtol without a solve (a start from
+    // the last solutions is solved to rtol)
+    sa.rtol_refine = P.warm_last ? P.rtol : P.refine_rtol;
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
@@ -398,7 +405,7 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     // start when it ran a refinement step (they then meet refine_rtol); a
     // request accepted on its prediction leaves the solved state in place,
     // so predictions do not drift from it
-    const bool store = in.outer_its > 0 || !warm;
+    const bool store = in.outer_its > 0 || !warm || P.warm_last;
     if (store) {
       for (size_t i = t; i < nu; i += SERVE_NT) __stcg(G.warm + i, u[i]);
       if (t < SERVE_K * 6) __stcg(G.warm_eps + t, seps[t]);
@@ -443,6 +450,7 @@ using namespace sp;
 
 struct sp_server_s {
   int ngeom = 0, dev = -1, grid = 0, cap = 0, running = 0;
+  long long launches = 0;  // launches of the loop (the first, and every relaunch)
   double last_alive = 0.0;  // host time of the last liveness check of the loop
   sp_server_opts o;
   std::vector<DevPlan *> plans;
@@ -486,6 +494,7 @@ extern "C" void sp_server_opts_default(sp_server_opts *o) {
   o->op = SP_OP_STENCIL;
   o->ctas_per_sm = 0;
   o->refine_rtol = 0.0;
+  o->warm_start = SP_WARM_PREDICT;
 }
 
 static int server_layout(int ngeom, const sp_rve_desc *descs, const sp_server_opts *o, int nsm,
@@ -564,6 +573,8 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   if (o.idle_spin_limit <= 0) o.idle_spin_limit = 2000000;
   if (o.op != SP_OP_ELL && o.op != SP_OP_STENCIL)
     return sp_set_error(SP_ERR_ARG, "sp_server_create: unknown operator");
+  if (o.warm_start != SP_WARM_PREDICT && o.warm_start != SP_WARM_LAST)
+    return sp_set_error(SP_ERR_ARG, "sp_server_create: unknown warm start");
   // the stencil solve of 7 load cases wants 128 registers (1 slot per SM)
   if (o.ctas_per_sm == 0) o.ctas_per_sm = (o.op == SP_OP_STENCIL) ? 1 : 2;
   if (o.ctas_per_sm != 1 && o.ctas_per_sm != 2)
@@ -713,6 +724,7 @@ extern "C" int sp_server_create(int ngeom, const sp_rve_desc *descs, const sp_se
   P.max_outer = 8;
   P.max_inner = 4000;
   P.idle_limit = o.idle_spin_limit;
+  P.warm_last = o.warm_start == SP_WARM_LAST;
   *out = s;
   return SP_OK;
 }
@@ -743,6 +755,7 @@ static int server_launch(sp_server *s) {
   serve_kernel(s->o)<<<s->grid, SERVE_NT, serve_dyn_smem(s->o), s->stream>>>(s->P);
   SP_CUDA_TRY(cudaGetLastError());
   s->running = 1;
+  s->launches++;
   return SP_OK;
 }
 
@@ -809,6 +822,20 @@ extern "C" int sp_server_poll(sp_server *s, long long ticket, double *stress, do
   if (info) *info = r.info;
   while (s->head_done < s->tail && s->h_res[s->head_done % s->cap].done == s->head_done + 1)
     s->head_done++;
+  return SP_OK;
+}
+
+extern "C" int sp_server_status(const sp_server *s, int *loop_on_device, long long *launches,
+                                long long *submitted) {
+  if (!s) return sp_set_error(SP_ERR_ARG, "null server");
+  if (loop_on_device) {
+    cudaError_t q = cudaStreamQuery(s->stream);
+    if (q != cudaSuccess && q != cudaErrorNotReady)
+      return sp_set_error(SP_ERR_CUDA, "serving loop failed: %s", cudaGetErrorString(q));
+    *loop_on_device = (q == cudaErrorNotReady);
+  }
+  if (launches) *launches = s->launches;
+  if (submitted) *submitted = s->tail;
   return SP_OK;
 }
 

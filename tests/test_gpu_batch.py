@@ -2,6 +2,8 @@
 batch against the oracle at the hot path's 1e-8 relative tolerance, in mixed
 (FP32 CG + FP64 refinement) and FP64 precision; results independent of the
 batch an RVE is solved in."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -66,11 +68,13 @@ def test_batch_custom_strains_and_materials(nrhs):
 
 
 def test_same_result_alone_and_in_mix():
+    """At a fixed CTA shape an RVE's result is bit-identical alone and in a
+    mix, and from launch to launch."""
     descs = make_descs(3, [6, 2, 8, 4, 6, 3, 5, 7, 2, 4] * 3)
-    big = mb.Batch(descs)
+    big = mb.Batch(descs, threads=512, ctas_per_sm=1)
     s_mix, _, _ = big.homogenize()
     for i in (0, 7, 19):
-        alone = mb.Batch([descs[i]])
+        alone = mb.Batch([descs[i]], threads=512, ctas_per_sm=1)
         s1, _, _ = alone.homogenize()
         assert np.array_equal(s1[0], s_mix[i])
     # and repeatable launch to launch
@@ -190,12 +194,19 @@ def test_periodic_rejects_assembled_operator_and_thin_meshes():
 
 
 def test_default_shape_per_operator():
+    """The fixed defaults, when the autotuner is off: 512 x 1 for the stencil
+    (128 registers a thread), 512 x 2 for the assembled operator."""
     descs = make_descs(2, [4, 5])
-    assert mb.Batch(descs).shape()[:2] == (512, 1)
-    assert mb.Batch(descs, op=mb.SP_OP_ELL).shape()[:2] == (512, 2)
-    assert mb.Batch(descs, bc=mb.SP_BC_PERIODIC).shape()[:2] == (512, 1)
-    assert mb.Batch(descs, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 1)
-    assert mb.Batch(descs, op=mb.SP_OP_ELL, precision=mb.SP_PREC_FP64).shape()[:2] == (512, 2)
+    off = mb.SP_TUNE_OFF
+    assert mb.Batch(descs, tune=off).shape()[:2] == (512, 1)
+    assert mb.Batch(descs, op=mb.SP_OP_ELL, tune=off).shape()[:2] == (512, 2)
+    assert mb.Batch(descs, bc=mb.SP_BC_PERIODIC, tune=off).shape()[:2] == (512, 1)
+    assert mb.Batch(descs, precision=mb.SP_PREC_FP64, tune=off).shape()[:2] == (512, 1)
+    assert mb.Batch(descs, op=mb.SP_OP_ELL, precision=mb.SP_PREC_FP64,
+                    tune=off).shape()[:2] == (512, 2)
+    assert mb.lib().sp_batch_create(2, (mb.sp_rve_desc * 2)(*descs),
+                                    C.byref(mb.batch_opts(tune=5)),
+                                    C.byref(mb._vp())) == mb.SP_ERR_ARG
 
 
 # --------------------------------------------------- edge and full sizes ---
@@ -290,3 +301,36 @@ def test_set_etype_rejects_bad_input():
         b.set_etype(1, np.zeros(27, np.uint8))
     with pytest.raises(mb.SputnikError):
         b.set_etype(0, np.full(27, 2, np.uint8))
+
+
+@pytest.mark.parametrize("op", [mb.SP_OP_STENCIL, mb.SP_OP_ELL])
+def test_autotuned_shape_is_measured_cached_and_correct(op):
+    """A batch whose shape is left open is timed on every instantiated CTA
+    shape; the fastest is launched, the choice is cached for the next batch
+    of the same kind, and results match the oracle; a batch whose shape is
+    given is not tuned."""
+    descs = make_descs(77, [9, 7, 9, 8, 6, 9, 5, 9] * 40)
+    a = mb.Batch(descs, op=op)
+    rep = a.tune_report()
+    assert rep and len(rep["candidates"]) >= 2
+    rates = [c["rate"] for c in rep["candidates"]]
+    best = rep["candidates"][int(np.argmax(rates))]
+    assert rep["chosen"] == {"threads": best["threads"], "ctas_per_sm": best["ctas_per_sm"]}
+    t, c, g = a.shape()
+    assert (t, c) == (best["threads"], best["ctas_per_sm"]) and g % c == 0
+    s, _, info = a.homogenize()
+    a.close()
+    assert (mb.info_array(info)["status"] == 0).all()
+    for i in (0, 1, 4):
+        st = oracle_stress(descs[i], np.eye(6))
+        assert np.abs(s[i] - st).max() <= 1e-8 * np.abs(st).max()
+    b = mb.Batch(descs, op=op)
+    rb = b.tune_report()
+    b.close()
+    assert rb["from_cache"] and rb["chosen"] == rep["chosen"]
+    fixed = mb.Batch(descs[:4], op=op, threads=512, ctas_per_sm=2)
+    assert fixed.tune_report() == {} and fixed.shape()[:2] == (512, 2)
+    fixed.close()
+    off = mb.Batch(descs[:4], op=op, tune=mb.SP_TUNE_OFF)
+    assert off.tune_report() == {}
+    off.close()

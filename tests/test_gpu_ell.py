@@ -133,8 +133,45 @@ def test_ell_dev_mvp_every_lane_width(lanes):
         yo = A.mvp(x)
         assert np.abs(y - yo).max() <= 1e-13 * np.abs(yo).max()
         assert mb.lib().sp_ell_dev_set_lanes(h, 3) == mb.SP_ERR_ARG
+        used = C.c_int()
+        mb.check(mb.lib().sp_ell_dev_lanes(h, C.byref(used), None, None), "lanes")
+        assert used.value == lanes if lanes else used.value in (4, 8, 16, 32)
     finally:
         mb.lib().sp_ell_dev_free(h)
+
+
+def test_ell_upload_autotunes_lanes_and_caches_the_choice():
+    """sp_ell_upload times every lanes-per-row width on the uploaded matrix
+    and keeps the fastest; a like matrix (same row width, same row-count
+    octave) takes the cached choice without a trial."""
+    m = O.cube_mesh(12)
+    et = O.fiber_types(m, [1, 1], 0.3)
+    A = O.assemble(m, et, (1e9, 2e10), (0.3, 0.2), symmetric_bc=True)
+    handles = []
+    try:
+        reports = []
+        for _ in range(2):
+            B = as_lib_matrix(A.cols.copy(), A.vals.copy())
+            h = mb._vp()
+            mb.check(mb.lib().sp_ell_upload(C.byref(B.m), C.byref(h)), "upload")
+            handles.append(h)
+            lanes, cached = C.c_int(), C.c_int()
+            us = (C.c_float * 4)()
+            mb.check(mb.lib().sp_ell_dev_lanes(h, C.byref(lanes), us, C.byref(cached)), "lanes")
+            reports.append((lanes.value, list(us), cached.value))
+        (l0, us0, c0), (l1, us1, c1) = reports
+        assert l0 in (4, 8, 16, 32) and all(t > 0 for t in us0)
+        # the chosen width is the fastest of the trial
+        assert us0[(4, 8, 16, 32).index(l0)] == min(us0)
+        assert c1 == 1 and l1 == l0 and us1 == us0
+        x = np.random.default_rng(3).standard_normal(m.ndof)
+        y = np.zeros(m.ndof)
+        mb.check(mb.lib().sp_ell_dev_mvp_host(handles[1], mb.ptr(x), mb.ptr(y)), "mvp")
+        yo = A.mvp(x)
+        assert np.abs(y - yo).max() <= 1e-13 * np.abs(yo).max()
+    finally:
+        for h in handles:
+            mb.lib().sp_ell_dev_free(h)
 
 
 def test_reference_unity_program_linked_to_library(golden_dir, tmp_path):

@@ -3,6 +3,7 @@ oracle's finite-difference tangent (micro/src/homogenize.c:59-94), the same
 request alone and in a mix of concurrent requests, the replay driver, and
 admission by HBM budget."""
 import ctypes as C
+import time
 
 import numpy as np
 import pytest
@@ -131,6 +132,58 @@ def test_repeated_and_zero_strain_requests_converge():
     assert np.abs(st0).max() <= 1e-9 * np.abs(st1).max()
     assert np.abs(tg0 - tg1).max() <= 1e-7 * np.abs(tg1).max()
     assert np.abs(tg0b - tg1).max() <= 1e-7 * np.abs(tg1).max()
+
+
+def test_warm_last_mode_solves_every_request():
+    """SP_WARM_LAST: each request starts from the geometry's last solution
+    of each load case (no prediction), runs CG to 1e-8, and keeps its
+    solution as the next start; results match the oracle."""
+    G = geoms()
+    s = mb.Server(G, warm_start=mb.SP_WARM_LAST)
+    s.start()
+    rng = np.random.default_rng(8)
+    reqs = [(g, rng.normal(0, 1e-3, 6)) for g in (2, 5, 2, 5, 2)]
+    res = [s.wait(s.submit(g, e)) for g, e in reqs]
+    s.stop()
+    s.close()
+    for (st, tg, info), (g, e) in zip(res, reqs):
+        assert info.status == 0 and info.relres <= 1e-8 and info.outer_its > 0
+        s0, Cm = oracle_fd(G[g], e)
+        assert np.abs(st - s0).max() <= 1e-8 * np.abs(s0).max()
+        assert np.abs(tg - Cm).max() <= 1e-7 * np.abs(Cm).max()
+    bad = mb.server_opts(warm_start=7)
+    descs = (mb.sp_rve_desc * len(G))(*G)
+    h = mb._vp()
+    assert mb.lib().sp_server_create(len(G), descs, C.byref(bad), C.byref(h)) == mb.SP_ERR_ARG
+
+
+def test_idle_loop_returns_and_is_relaunched():
+    """Every device wait of the serving loop is bounded: with a small
+    idle_spin_limit the loop returns by itself once its queue stays empty
+    (the host sees its stream idle), and the next submit relaunches it; the
+    answers before and after match the oracle."""
+    G = geoms()
+    s = mb.Server(G, idle_spin_limit=1000)
+    s.start()
+    e1 = np.array([3e-4, -1e-4, 2e-4, 0.0, 1e-4, -2e-4])
+    st1, tg1, i1 = s.wait(s.submit(1, e1))
+    deadline = time.time() + 20.0
+    on, n1, _ = s.status()
+    while on and time.time() < deadline:
+        time.sleep(0.01)
+        on, n1, _ = s.status()
+    assert not on and n1 == 1
+    e2 = np.array([-2e-4, 4e-4, 1e-4, 2e-4, 0.0, 1e-4])
+    st2, tg2, i2 = s.wait(s.submit(3, e2))
+    _, n2, sub = s.status()
+    s.stop()
+    s.close()
+    assert n2 == 2 and sub == 2
+    for st, tg, info, g, e in ((st1, tg1, i1, 1, e1), (st2, tg2, i2, 3, e2)):
+        assert info.status == 0 and info.relres <= 1e-8
+        s0, Cm = oracle_fd(G[g], e)
+        assert np.abs(st - s0).max() <= 1e-8 * np.abs(s0).max()
+        assert np.abs(tg - Cm).max() <= 1e-7 * np.abs(Cm).max()
 
 
 # --------------------------------------- message_t coupling (micro side) ---
