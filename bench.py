@@ -65,8 +65,10 @@ def algorithmic_bytes(sizes, inner_its, outer_its, k=6, stencil=True):
     FP32 matrix values (4 B per structural nonzero) and one int32 column node
     per 3x3 block (the node-sliced ELL stores one per block), or, for the
     stencil operator, one material byte per element; and 8 FP32 vector
-    passes.  Per refinement step 3 FP64 vector passes.  Once per RVE the
-    assembled values (written) or the stencil's Jacobi diagonal."""
+    passes.  Per refinement step 3 FP64 vector passes, plus one for the
+    residual of the boundary values alone (the right-hand side the stopping
+    rule is relative to; the solve starts from the affine field).  Once per
+    RVE the assembled values (written) or the stencil's Jacobi diagonal."""
     total = 0.0
     for n, it, ot in zip(sizes, inner_its, outer_its):
         n, it, ot = int(n), float(it), float(ot)
@@ -80,7 +82,7 @@ def algorithmic_bytes(sizes, inner_its, outer_its, k=6, stencil=True):
             setup = nelm * (576 * 4 + 24 * 4)
         vec = 8 * k * ndof * 4
         refine = 3 * k * ndof * 8
-        total += it * (spmm + vec) + (ot + 1) * refine + setup
+        total += it * (spmm + vec) + (ot + 2) * refine + setup
     return total
 
 

@@ -296,8 +296,9 @@ typedef struct {
                            meet rtol without a solve (0: rtol / 100) */
   int warm_start;       /* SP_WARM_PREDICT (default): first-order prediction from the
                            geometry's last solved request; SP_WARM_LAST: each load case
-                           starts from the geometry's last solution of that load case, and
-                           every request is solved to rtol and kept as the next start */
+                           starts from the geometry's last solution of that load case,
+                           shifted by the affine field of the strain difference, and every
+                           request is solved to rtol and kept as the next start */
 } sp_server_opts;
 #define SP_WARM_PREDICT 0
 #define SP_WARM_LAST 1

@@ -219,15 +219,16 @@ __device__ inline void bc_and_dinv(int t, int nt, const MeshGeo &g, const int *_
 // ------------------------------------------------------------ load cases ---
 
 // u = eps . x on boundary dofs (micro/src/homogenize.c:227-242, 335-342 in
-// 3D), zero elsewhere; eps[k][6] Voigt with engineering shears.
+// 3D), zero elsewhere -- or, with `inside`, eps . x at every node (the
+// homogeneous affine start iterate); eps[k][6] Voigt with engineering shears.
 template <int K>
 __device__ inline void affine_init(int t, int nt, const MeshGeo &g, const double *eps, int nrhs,
-                                   double *u) {
+                                   double *u, bool inside = false) {
   for (int x = t; x < g.ndof * K; x += nt) {
     int dof = x / K, k = x % K;
     int node = dof / 3, d = dof % 3;
     double val = 0.0;
-    if (k < nrhs && is_bnode(g, node)) {
+    if (k < nrhs && (inside || is_bnode(g, node))) {
       int i = node % g.nx, j = (node / g.nx) % g.ny, kk = node / (g.nx * g.ny);
       double X = i * g.hx, Y = j * g.hy, Z = kk * g.hz;
       const double *e = eps + k * 6;
@@ -1122,130 +1123,6 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
   }
 }
 
-// The FP32 Dirichlet stencil SpMM of spmm_stencil_xw with the x-neighbour
-// exchange moved from the inputs to the outputs.  The operator is
-// symmetric, so the dx = -1 term of node i+1, B_{i+1}(-1, dy, dz) x_{i +
-// (0, dy, dz)}, multiplies the value lane i gathered for its own column: lane
-// i forms it with lane i+1's block (pattern from lane i+1's material mask)
-// and likewise the dx = +1 term of node i-1.  The three sums are kept apart
-// over all 9 (dy, dz) rows and the neighbours' parts cross lanes once per
-// warp trip (2 x 3K shuffles instead of 2 x 3K per row); a lane adds the
-// part from lane i-1 (i+1) only when that lane holds its x-neighbour, i.e.
-// unless its node is first (last) in its x-row of interior nodes.
-template <int K>
-__device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const float *KB,
-                                       const uint8_t *__restrict__ etype, const float *x,
-                                       float *y, double *dot, unsigned amask, bool rev) {
-  constexpr int KP = (K + 1) / 2;
-  constexpr unsigned FULL = 0xffffffffu;
-  const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
-  const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
-  const int ni = mx * my * mz;
-  const int sy = g.nx, sz = g.nx * g.ny;
-  const int esy = g.nex, esz = g.nex * g.ney;
-  const size_t blk = (size_t)3 * g.nn_pad;
-  const int ngr = (ni + 29) / 30;
-  for (int gi = warp; gi < ngr; gi += nwarps) {
-    const int s0 = (rev ? ngr - 1 - gi : gi) * 30;
-    const int id = s0 - 1 + lane;
-    const bool out = lane >= 1 && lane <= 30 && id < ni;
-    const int idc = min(max(id, 0), ni - 1);
-    const int ii = idc % mx, jj = (idc / mx) % my, kk = idc / (mx * my);
-    const int i = ii + 1, j = jj + 1, k = kk + 1;
-    const int a = i + j * sy + k * sz;
-    const bool lo = ii > 0, hi = ii < mx - 1;
-    unsigned mask = 0;
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
-      const int e = (i - 1 + ox) + (j - 1 + oy) * esy + (k - 1 + oz) * esz;
-      mask |= (unsigned)__ldg(etype + e) << c;
-    }
-    const unsigned mr = __shfl_down_sync(FULL, mask, 1);  // lane i+1's materials
-    const unsigned ml = __shfl_up_sync(FULL, mask, 1);    // lane i-1's materials
-    float2 acc[3][KP], accr[3][KP], accl[3][KP];
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-#pragma unroll
-      for (int p = 0; p < KP; p++)
-        acc[d][p] = accr[d][p] = accl[d][p] = make_float2(0.f, 0.f);
-#pragma unroll 1
-    for (int dz = -1; dz <= 1; dz++) {
-#if defined(SP_XO_ROW1)
-#pragma unroll 1
-#else
-#pragma unroll
-#endif
-      for (int dy = -1; dy <= 1; dy++) {
-        const float *xb = x + nbk_base<K>(a + dy * sy + dz * sz);
-        float2 xv[3][KP];
-#pragma unroll
-        for (int p = 0; p < KP; p++)
-#pragma unroll
-          for (int c = 0; c < 3; c++) {
-            xv[c][p] = make_float2(0.f, 0.f);
-            if ((amask >> (2 * p)) & 3u) {
-              xv[c][p].x = xb[(c * K + 2 * p) * 32];
-              if (2 * p + 1 < K) xv[c][p].y = xb[(c * K + 2 * p + 1) * 32];
-            }
-          }
-        // own block (dx = 0), lane i+1's dx = -1 block, lane i-1's dx = +1 block
-#pragma unroll
-        for (int w = 0; w < 3; w++) {
-          const int idx = w == 0 ? sp_pt_index(mask, 0, dy, dz)
-                                 : (w == 1 ? sp_pt_index(mr, -1, dy, dz) : sp_pt_index(ml, 1, dy, dz));
-          float bv[9] = {};
-          add_block<float, float>(KB + idx * SP_PT_REC, bv);
-          float2 (&ac)[3][KP] = w == 0 ? acc : (w == 1 ? accr : accl);
-#pragma unroll
-          for (int p = 0; p < KP; p++) {
-            if (!((amask >> (2 * p)) & 3u)) continue;
-#pragma unroll
-            for (int d = 0; d < 3; d++)
-#pragma unroll
-              for (int c = 0; c < 3; c++) {
-                const float b = bv[d * 3 + c];
-                ac[d][p] = __ffma2_rn(make_float2(b, b), xv[c][p], ac[d][p]);
-              }
-          }
-        }
-      }
-    }
-    // the neighbours' parts: lane i-1's accr and lane i+1's accl
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-#pragma unroll
-      for (int p = 0; p < KP; p++) {
-        if (!((amask >> (2 * p)) & 3u)) continue;
-        float2 fl, fr;
-        fl.x = __shfl_up_sync(FULL, accr[d][p].x, 1);
-        fl.y = __shfl_up_sync(FULL, accr[d][p].y, 1);
-        fr.x = __shfl_down_sync(FULL, accl[d][p].x, 1);
-        fr.y = __shfl_down_sync(FULL, accl[d][p].y, 1);
-        if (lo) {
-          acc[d][p].x += fl.x;
-          acc[d][p].y += fl.y;
-        }
-        if (hi) {
-          acc[d][p].x += fr.x;
-          acc[d][p].y += fr.y;
-        }
-      }
-    if (out) {
-#pragma unroll
-      for (int q = 0; q < K; q++) {
-        if (!((amask >> q) & 1u)) continue;
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          const float yv = (q & 1) ? acc[d][q >> 1].y : acc[d][q >> 1].x;
-          dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
-          y[q * blk + (size_t)d * g.nn_pad + a] = yv;
-        }
-      }
-    }
-  }
-}
-
 // b = -K u on interior dofs in stencil form (Dirichlet conditions): one
 // thread per interior dof row, the row of each of the node's 27 assembled
 // 3x3 blocks (FP64, summed from the element blocks of its 8 elements,
@@ -1253,7 +1130,9 @@ __device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const fl
 // included; 0 on boundary and padding dofs.  The same sums as residual_soa in
 // another order, with 27 instead of 64 neighbour reads per row.  SCALE: adds
 // the squared norm of the rows' sums of term magnitudes into scale2[K].
-template <int K, typename R, bool SCALE = false>
+// BCONLY: u's interior values are read as 0, giving the right-hand side
+// -K u_bc of the load cases whatever u holds inside.
+template <int K, typename R, bool SCALE = false, bool BCONLY = false>
 __device__ inline void residual_stencil(int t, int nt, const MeshGeo &g,
                                         const uint8_t *__restrict__ etype,
                                         const double *KBd /*stencil tables, shared*/,
@@ -1317,11 +1196,14 @@ __device__ inline void residual_stencil(int t, int nt, const MeshGeo &g,
           }
         }
         const int nb = a + dx + dy * sy + dz * sz;
+        // (BCONLY) whether the neighbour is a boundary node
+        const bool nbb = !BCONLY || i + dx == 0 || i + dx == g.nx - 1 || j + dy == 0 ||
+                         j + dy == g.ny - 1 || k + dz == 0 || k + dz == g.nz - 1;
 #pragma unroll
         for (int q = 0; q < K; q++)
 #pragma unroll
           for (int c = 0; c < 3; c++) {
-            const double uv = u[q * blk + (size_t)c * g.nn_pad + nb];
+            const double uv = nbb ? u[q * blk + (size_t)c * g.nn_pad + nb] : 0.0;
             acc[q] = fma(bv[c], uv, acc[q]);
             if (SCALE) mag[q] += fabs(bv[c] * uv);
           }
@@ -1635,10 +1517,13 @@ __device__ inline void residual_soa(int t, int nt, const MeshGeo &g,
 }
 
 // u = eps . x on boundary dofs; interior dofs are set to 0 (keep_inside =
-// false) or kept (warm start); load cases >= nrhs and padding are 0.
+// false) or kept (warm start), or (affine_inside) set to eps . x as well --
+// the homogeneous affine field, the exact solution for a homogeneous RVE and
+// a start iterate whose error in a composite lies near the material
+// interfaces; load cases >= nrhs and padding are 0.
 template <int K>
 __device__ inline void affine_soa(int t, int nt, const MeshGeo &g, const double *eps, int nrhs,
-                                  bool keep_inside, double *u) {
+                                  bool keep_inside, double *u, bool affine_inside = false) {
   const size_t blk = (size_t)3 * g.nn_pad;
   for (size_t x = t; x < K * blk; x += nt) {
     int k = (int)(x / blk);
@@ -1648,7 +1533,7 @@ __device__ inline void affine_soa(int t, int nt, const MeshGeo &g, const double 
       u[x] = 0.0;
       continue;
     }
-    if (!is_bnode(g, node)) {
+    if (!affine_inside && !is_bnode(g, node)) {
       if (!keep_inside) u[x] = 0.0;
       continue;
     }

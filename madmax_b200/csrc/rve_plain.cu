@@ -47,8 +47,9 @@ __global__ void k_bc(MeshGeo g, const int *cols, T *vals, T *dinv) {
 }
 
 template <int K>
-__global__ void k_affine(MeshGeo g, const double *eps, int nrhs, double *u) {
-  affine_init<K>(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, g, eps, nrhs, u);
+__global__ void k_affine(MeshGeo g, const double *eps, int nrhs, double *u, bool inside) {
+  affine_init<K>(blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, g, eps, nrhs, u,
+                 inside);
 }
 
 // b = -K u (interior), 0 (boundary); norms[k] = ||b_k||^2
@@ -306,11 +307,16 @@ static int rve_solve_k(sp_rve *r, Device *d, PcgGraph<double, K, 32> *&pcg, int 
   double eps[KMAX * 6] = {0};
   memcpy(eps, strains, (size_t)nrhs * 6 * sizeof(double));
   SP_CUDA_TRY(cudaMemcpyAsync(r->d_eps, eps, sizeof(eps), cudaMemcpyHostToDevice, s));
-  k_affine<K><<<nb_vec, 256, 0, s>>>(g, r->d_eps, nrhs, r->d_u);
+  k_affine<K><<<nb_vec, 256, 0, s>>>(g, r->d_eps, nrhs, r->d_u, false);
   launches++;
   double r0[KMAX] = {0}, rn[KMAX] = {0};
   int outer = 0, inner = 0, max_outer = 6;
-  // Newton / refinement: b = -K u, solve A x = b, u += x  (micro/src/homogenize.c:184-215)
+  bool started = false;
+  // Newton / refinement: b = -K u, solve A x = b, u += x  (micro/src/homogenize.c:184-215).
+  // The first residual, of the boundary values alone, is the right-hand side
+  // the stopping rule is relative to; the iteration then starts from the
+  // homogeneous affine field eps . x inside (the exact solution for a
+  // homogeneous RVE), which leaves the error near the material interfaces.
   for (;;) {
     double nrm[KMAX];
     k_residual<K><<<nb_node, 256, 0, s>>>(g, r->d_etype, r->d_Ke, r->d_u, r->d_b, r->d_out + 8 * 12,
@@ -318,16 +324,24 @@ static int rve_solve_k(sp_rve *r, Device *d, PcgGraph<double, K, 32> *&pcg, int 
     launches++;
     SP_CUDA_TRY(cudaMemcpyAsync(nrm, r->d_out + 8 * 12, K * sizeof(double), cudaMemcpyDeviceToHost, s));
     SP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (!started) {
+      for (int k = 0; k < nrhs; k++) r0[k] = sqrt(nrm[k]);
+      k_affine<K><<<nb_vec, 256, 0, s>>>(g, r->d_eps, nrhs, r->d_u, true);
+      launches++;
+      started = true;
+      continue;
+    }
     bool done = true;
     for (int k = 0; k < nrhs; k++) {
       rn[k] = sqrt(nrm[k]);
-      if (outer == 0) r0[k] = rn[k];
       if (r0[k] > 0 && rn[k] > rtol * r0[k]) done = false;
     }
     if (done || outer >= max_outer) break;
     PcgState st0 = {};
     st0.nactive = nrhs;
-    st0.rtol2 = (0.5 * rtol) * (0.5 * rtol);
+    // each correction to a quarter of the target (the margin of the batch's
+    // corrections, rve_solve.cuh)
+    st0.rtol2 = (0.25 * rtol) * (0.25 * rtol);
     st0.max_its = 20000;
     SP_CUDA_TRY(cudaMemcpyAsync(r->d_st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
     int fixed = 0;

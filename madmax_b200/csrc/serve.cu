@@ -343,8 +343,26 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
       srn0[t] = sqrt(fmax(s, 0.0));
     }
     if (warm && P.warm_last) {
-      // the last request's solution of each load case, as it is
-      for (size_t i = t; i < nu; i += SERVE_NT) u[i] = __ldcg(G.warm + i);
+      // the last request's solution of each load case, shifted by the affine
+      // field of the strain difference: u_last + (eps - eps_last) . x (the
+      // boundary values become eps . x; exact for a homogeneous RVE, and
+      // close when consecutive strains on a geometry are close)
+      const size_t blk = (size_t)3 * g.nn_pad;
+      for (size_t i = t; i < nu; i += SERVE_NT) {
+        const int k = (int)(i / blk), rem = (int)(i % blk);
+        const int d = rem / g.nn_pad, node = rem % g.nn_pad;
+        double v = __ldcg(G.warm + i);
+        if (node < g.nn) {
+          const int ix = node % g.nx, iy = (node / g.nx) % g.ny, iz = node / (g.nx * g.ny);
+          double de[6];
+          for (int c = 0; c < 6; c++) de[c] = seps[k * 6 + c] - __ldcg(G.warm_eps + k * 6 + c);
+          const double X = ix * g.hx, Y = iy * g.hy, Z = iz * g.hz;
+          v += d == 0 ? de[0] * X + 0.5 * de[3] * Y + 0.5 * de[5] * Z
+                      : (d == 1 ? 0.5 * de[3] * X + de[1] * Y + 0.5 * de[4] * Z
+                                : 0.5 * de[5] * X + 0.5 * de[4] * Y + de[2] * Z);
+        }
+        u[i] = v;
+      }
     } else if (warm) {
       if (t < SERVE_K * 6) {
         const int k = t / 6, j = t % 6;
@@ -374,7 +392,9 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     else if constexpr (STENCIL)
       stencil_blocks<float>(t, SERVE_NT, sKe, sKB);
     stencil_blocks<double>(t, SERVE_NT, sKe, sKBd);
-    affine_soa<SERVE_K>(t, SERVE_NT, g, seps, SERVE_NRHS, warm, u);
+    // a cold request (no earlier solution on this geometry) starts from the
+    // homogeneous affine field inside; a warm one keeps its start inside
+    affine_soa<SERVE_K>(t, SERVE_NT, g, seps, SERVE_NRHS, warm, u, !warm);
     __syncthreads();
     SolveArgs sa;
     sa.nrhs = SERVE_NRHS;
@@ -386,7 +406,7 @@ __global__ void __launch_bounds__(SERVE_NT, MINB) k_serve(ServeParams P) {
     sa.inner_rtol = P.inner_rtol;
     sa.max_outer = P.max_outer;
     sa.max_inner = P.max_inner;
-    sa.warm = warm;
+    sa.warm = 1;  // every start iterate is measured against the right-hand side's norm
     sa.rn0_given = srn0;
     sa.kbd = sKBd;
     sa.eps = nullptr;  // affine conditions: eps is carried by u's boundary values
