@@ -109,13 +109,13 @@ def argv_tail(args):
 # bench cannot count DRAM bytes itself, so a run whose workload differs
 # reports null.
 PROFILED_TRAFFIC = {
-    # k_batch, stencil operator: ncu --metrics dram__bytes_read.sum,
+    # k_batch, stencil operator, autotuned shape: ncu --metrics dram__bytes_read.sum,
     # dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
-    # -k regex:k_batch -s 3 -c 1 python bench.py --steps 1 --warmup 3 ...
+    # -k regex:k_batch -s 13 -c 1 python bench.py --steps 1 --warmup 3 ...
     "k_batch --nrve 4096 --sizes 8 12 16 20 --op stencil --threads 0 --ctas 0 "
-    "--inner-rtol 0.0001": 1039010537728,
+    "--inner-rtol 0.0001": 686171300096,
     # k_spmv_rve, the n = 40 structured matrix, cold L2
-    "k_spmv_rve structured ELL n=40": 218744832,
+    "k_spmv_rve structured ELL n=40": 214213376,
 }
 
 
@@ -294,12 +294,12 @@ def _oracle_rve(args):
     return int(n), time.perf_counter() - t
 
 
-def cpu_sample(nrve_sample: int, seed: int, procs: int):
-    """Time the oracle (FP64 Jacobi-PCG, 6 load cases) on a sample of the
-    workload; returns seconds per RVE for each mesh size."""
-    n, radius, ratio, nu_m, nu_f = workload_params(nrve_sample, seed)
-    work = [(n[i], radius[i], ratio[i], nu_m[i], nu_f[i]) for i in range(nrve_sample)]
-    work.sort(key=lambda w: -w[0])  # largest first keeps the pool busy to the end
+def cpu_sample(work, procs: int):
+    """Time the oracle (FP64 Jacobi-PCG from the reference's zero start, 6
+    load cases) on RVEs of the workload, given as (n, radius, ratio, nu_m,
+    nu_f) tuples; returns seconds per RVE for each mesh size, the wall time
+    and the per-RVE results."""
+    work = sorted(work, key=lambda w: -w[0])  # largest first keeps the pool busy to the end
     if procs > 1:
         import multiprocessing as mp
         with mp.get_context("spawn").Pool(procs) as pool:
@@ -313,6 +313,22 @@ def cpu_sample(nrve_sample: int, seed: int, procs: int):
         wall = time.perf_counter() - t0
     per = {s: [t for (nn, t) in res if nn == s] for s in SIZES}
     return per, wall, res
+
+
+def workload_items(nrve: int, seed: int, sizes=SIZES):
+    """The workload's RVEs as (n, radius, ratio, nu_m, nu_f) tuples, in the
+    order the GPU arm builds them."""
+    n, radius, ratio, nu_m, nu_f = workload_params(nrve, seed, sizes)
+    return [(int(n[i]), float(radius[i]), float(ratio[i]), float(nu_m[i]), float(nu_f[i]))
+            for i in range(nrve)]
+
+
+def per_size_sample(items, per_size: int):
+    """The first `per_size` RVEs of every mesh size."""
+    out = []
+    for s_ in sorted(set(w[0] for w in items)):
+        out += [w for w in items if w[0] == s_][:per_size]
+    return out
 
 
 def mix_rate(per_size_times):
@@ -382,12 +398,15 @@ def run_reference(args):
     O.lib()
     cores = os.cpu_count() or 1
     per_step = 4 * cores  # RVEs per step: four per core, so the pool stays busy
+    # the GPU arm's own RVEs (rank 0's seed), a bounded slice per step
+    items = workload_items(args.nrve, rank_seed(0), tuple(args.sizes))
     for _ in range(args.warmup):
-        cpu_sample(min(per_step, 4), 999, min(cores, 4))
+        cpu_sample(items[:min(cores, 4)], min(cores, 4))
     rates = []
     t_all = 0.0
     for k in range(args.steps):
-        per, wall, res = cpu_sample(per_step, 2024 + k, cores)
+        sl = [items[(k * per_step + j) % len(items)] for j in range(per_step)]
+        per, wall, res = cpu_sample(sl, cores)
         rates.append(len(res) / wall)
         t_all += wall
     value = float(np.mean(rates))
@@ -400,8 +419,9 @@ def run_reference(args):
                    "sample_rves_per_step": per_step, "solver": "FP64 Jacobi-PCG (oracle port)",
                    "parallelism": f"rank 0 of {args.gpus}: all host cores"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{per_step} seeded RVEs of the workload mix per step, "
-                                   f"spawned process pool, one process per core"},
+                         "sample": f"{per_step} consecutive RVEs of the GPU arm's own "
+                                   f"{args.nrve}-RVE workload per step (step k takes RVEs "
+                                   f"k*{per_step} on), spawned process pool, one process per core"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -555,11 +575,13 @@ def run_ours(args):
         if world == 1 and not args.no_fe2:
             line["fe2"] = fe2_step(mb, args)
         if world == 1 and not args.no_cpu:
-            per, wall, res = cpu_sample(args.cpu_sample, 77, 1)
+            items = workload_items(args.nrve, rank_seed(rank), tuple(args.sizes))
+            per, wall, res = cpu_sample(per_size_sample(items, args.cpu_sample), 1)
             line["cpu_baseline"] = {
                 "value": mix_rate(per), "unit": UNIT, "cores": 1, "kind": "port",
-                "sample": f"{len(res)} seeded RVEs of the workload mix, FP64 Jacobi-PCG oracle "
-                          f"on 1 core ({wall:.1f} s), rate = 1 / mean over sizes of s per RVE"}
+                "sample": f"{len(res)} RVEs of the timed workload ({args.cpu_sample} of each size), "
+                          f"FP64 Jacobi-PCG oracle from the reference's zero start on 1 core "
+                          f"({wall:.1f} s), rate = 1 / mean over sizes of s per RVE"}
     batch.close()
     if dist:
         dist.barrier()
@@ -818,7 +840,8 @@ def main(argv=None):
                     help="RVEs per mesh size checked against the oracle after timing")
     ap.add_argument("--no-ell", action="store_true",
                     help="skip the assembled-ELL batched rate on the same mix")
-    ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--cpu-sample", type=int, default=2,
+                    help="RVEs of each mesh size timed on the CPU oracle (1 core)")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
