@@ -97,10 +97,8 @@ static int shape_setup(const sp_batch_opts &o, int kp, const Device *d, const Sh
                         "cluster %d, %s operator in this precision", sh.threads, sh.ctas,
                         sh.cluster, o.op == SP_OP_ELL ? "assembled" : "stencil");
   int g = d->nsm * sh.ctas;
-  const int dyn = sp_batch_uses_ptable(o.precision == SP_PREC_MIXED, kp, sh.op,
-                                       sh.threads * sh.ctas <= 512)
-                      ? SP_PT_BYTES
-                      : 0;
+  const int dyn = sp_batch_dyn_smem(o.precision == SP_PREC_MIXED, kp, sh.op,
+                                    sh.threads * sh.ctas <= 512);
   if (dyn && cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   dyn) != cudaSuccess) {
     cudaGetLastError();

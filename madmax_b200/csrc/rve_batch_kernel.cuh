@@ -20,6 +20,11 @@ __host__ __device__ constexpr bool sp_batch_uses_ptable(bool fp32, int K, int op
   return op == SP_OP_STENCIL && fp32 && (K <= 6 || wide);
 }
 
+// Dynamic shared memory of a k_batch variant: the pattern table or nothing.
+__host__ __device__ constexpr int sp_batch_dyn_smem(bool fp32, int K, int op, bool wide) {
+  return sp_batch_uses_ptable(fp32, K, op, wide) ? SP_PT_BYTES : 0;
+}
+
 struct BatchPlan {
   MeshGeo geo; // node/element counts; h and vol per RVE
   const int *cols;

@@ -72,6 +72,16 @@ struct CgShared {
   int phase;
 };
 
+// The right-hand side of the boundary values alone and its norms, once per
+// RVE: kept out of line, so that its registers do not add to the CG loop's.
+template <int K, typename T>
+__device__ __noinline__ void rhs_stencil(int gt, int gnt, const MeshGeo &g,
+                                         const uint8_t *__restrict__ etype, const double *kbd,
+                                         const double *__restrict__ u, T *r, double *nrm2,
+                                         double *scale2) {
+  residual_stencil<K, T, true, true>(gt, gnt, g, etype, kbd, u, r, nrm2, scale2);
+}
+
 // Barrier over the threads that solve one RVE.
 template <int CL>
 __device__ inline void rve_sync() {
@@ -226,7 +236,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
 #pragma unroll
     for (int k = 0; k < 2 * K; k++) m0[k] = 0.0;
     if (P.kbd)  // Dirichlet stencil tables: 27 instead of 64 neighbour reads per row
-      residual_stencil<K, T, true, true>(gt, GNT, g, etype, P.kbd, u, r, m0, m0 + K);
+      rhs_stencil<K, T>(gt, GNT, g, etype, P.kbd, u, r, m0, m0 + K);
     else
       residual_soa<K, T, true, true>(gt, GNT, g, etype, sKe, u, r, m0, m0 + K);
     rve_reduce<2 * K, CL>(m0, red, sh);

@@ -81,3 +81,17 @@ def test_reference_arm_line_matches_our_config():
     assert line["unit"] == bench.UNIT and line["higher_is_better"] is True
     assert line["config"]["workload"].startswith("batched tangent: 4096 RVEs per GPU")
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+
+
+def test_reference_arm_samples_the_gpu_arms_rves():
+    """The CPU arm and the CPU baseline time RVEs of the GPU arm's own
+    workload (same seed, same parameters), not a separate draw."""
+    import madmax_b200 as mb
+    items = bench.workload_items(64, bench.rank_seed(0))
+    descs = bench.workload_descs(mb, 64, bench.rank_seed(0))
+    for it, d in zip(items, descs):
+        assert it[0] == d.n[0] and it[1] == d.radius
+        assert d.E[1] == bench.E_MATRIX * it[2] and (d.nu[0], d.nu[1]) == (it[3], it[4])
+    sample = bench.per_size_sample(items, 2)
+    assert len(sample) == 8 and sorted({w[0] for w in sample}) == [8, 12, 16, 20]
+    assert all(w in items for w in sample)
