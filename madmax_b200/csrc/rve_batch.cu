@@ -210,7 +210,7 @@ struct sp_batch_s {
   double *d_strains = nullptr, *d_mats = nullptr, *d_stress = nullptr, *d_strain = nullptr;
   sp_solve_info *d_info = nullptr;
   double *d_ws_u = nullptr;
-  void *d_ws_v = nullptr, *d_ws_rm = nullptr, *d_ws_drm = nullptr, *d_ws_dinv = nullptr;
+  void *d_ws_v = nullptr, *d_ws_dinv = nullptr;
   size_t bytes = 0;
   TuneRecord tune;  // the autotuner's trial (tune.n == 0: shape fixed by the caller)
   int tune_slots = 0;  // work spaces allocated while the autotuner runs
@@ -312,7 +312,7 @@ extern "C" int sp_batch_destroy(sp_batch *b) {
   if (!b) return SP_OK;
   void *bufs[] = {b->d_plans, b->d_rves, b->d_order, b->d_counter, b->d_vals, b->d_dinv,
                   b->d_etype, b->d_strains, b->d_mats, b->d_stress, b->d_strain, b->d_info,
-                  b->d_ws_u, b->d_ws_v, b->d_ws_rm, b->d_ws_drm, b->d_ws_dinv};
+                  b->d_ws_u, b->d_ws_v, b->d_ws_dinv};
   for (void *p : bufs) cudaFree(p);
   for (DevPlan *p : b->plans) plan_release(p);
   delete b;
@@ -494,7 +494,7 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   }
   size_t stride = (size_t)kp * 3 * maxnp;
   // (3*maxnp >= maxdof; a multiple of 96, so every slot starts 16-byte aligned)
-  size_t rm_stride = (size_t)maxdof * SP_WP, drm_stride = (size_t)3 * maxnp;
+  size_t drm_stride = (size_t)3 * maxnp;
   const bool ell = o.op == SP_OP_ELL;
   size_t *acct = &b->bytes;
   if (!rc) rc = dmalloc((void **)&b->d_plans, hplans.size() * sizeof(BatchPlan), acct);
@@ -513,8 +513,6 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   const size_t slots = (size_t)std::max(b->grid / o.cluster, b->tune_slots);
   if (!rc) rc = dmalloc((void **)&b->d_ws_u, slots * stride * sizeof(double), acct);
   if (!rc) rc = dmalloc(&b->d_ws_v, slots * 4 * stride * tsz, acct);
-  if (!rc && ell) rc = dmalloc(&b->d_ws_rm, slots * rm_stride * tsz, acct);
-  if (!rc && ell) rc = dmalloc(&b->d_ws_drm, slots * drm_stride * tsz, acct);
   // stencil: one Jacobi diagonal [3][max nn_pad] per work space
   if (!rc && !ell) rc = dmalloc(&b->d_ws_dinv, slots * drm_stride * tsz, acct);
   if (!rc) {
@@ -558,9 +556,6 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   P.ws_u = b->d_ws_u;
   P.ws_v = b->d_ws_v;
   P.ws_stride = stride;
-  P.ws_rm = b->d_ws_rm;
-  P.ws_drm = b->d_ws_drm;
-  P.rm_stride = rm_stride;
   P.drm_stride = drm_stride;
   P.ws_dinv = b->d_ws_dinv;
   P.counter = b->d_counter;
@@ -586,22 +581,15 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
     if (!rc && keep < slots) {
       cudaFree(b->d_ws_u);
       cudaFree(b->d_ws_v);
-      cudaFree(b->d_ws_rm);
-      cudaFree(b->d_ws_drm);
       cudaFree(b->d_ws_dinv);
       b->d_ws_u = nullptr;
-      b->d_ws_v = b->d_ws_rm = b->d_ws_drm = b->d_ws_dinv = nullptr;
-      b->bytes -= slots * (stride * sizeof(double) + 4 * stride * tsz +
-                           (ell ? rm_stride * tsz + drm_stride * tsz : drm_stride * tsz));
+      b->d_ws_v = b->d_ws_dinv = nullptr;
+      b->bytes -= slots * (stride * sizeof(double) + 4 * stride * tsz + (ell ? 0 : drm_stride * tsz));
       if (!rc) rc = dmalloc((void **)&b->d_ws_u, keep * stride * sizeof(double), acct);
       if (!rc) rc = dmalloc(&b->d_ws_v, keep * 4 * stride * tsz, acct);
-      if (!rc && ell) rc = dmalloc(&b->d_ws_rm, keep * rm_stride * tsz, acct);
-      if (!rc && ell) rc = dmalloc(&b->d_ws_drm, keep * drm_stride * tsz, acct);
       if (!rc && !ell) rc = dmalloc(&b->d_ws_dinv, keep * drm_stride * tsz, acct);
       P.ws_u = b->d_ws_u;
       P.ws_v = b->d_ws_v;
-      P.ws_rm = b->d_ws_rm;
-      P.ws_drm = b->d_ws_drm;
       P.ws_dinv = b->d_ws_dinv;
     }
     b->tune_slots = 0;

@@ -56,9 +56,6 @@ struct BatchParams {
   double *ws_u;          // per CTA [K][3][max nn_pad] FP64
   void *ws_v;            // per CTA 4 x [K][3][max nn_pad] of T: r, x, p, q
   size_t ws_stride;      // K*3*max nn_pad
-  void *ws_rm;           // per CTA row-major assembly scratch [maxdof][84] of T
-  void *ws_drm;          // per CTA row-major diagonal scratch [maxdof] of T
-  size_t rm_stride;      // maxdof*84
   size_t drm_stride;     // 3*max nn_pad
   void *ws_dinv;         // stencil operator: per CTA Jacobi diagonal [3][max nn_pad] of T
   int *counter;
@@ -77,8 +74,8 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   // FP64 stencil tables for the residual (an FP64 stencil batch has them in sKeT already)
   constexpr bool OWN_KBD = !PER && !(STENCIL && sizeof(T) == 8);
   __shared__ __align__(16) double sKBd[OWN_KBD ? SP_KB_SIZE : 2];
-  // element scatter values (assembled operator) or element blocks (stencil)
-  __shared__ __align__(16) T sKeT[STENCIL ? (PT ? 4 : SP_KB_SIZE) : 2 * SP_KE];
+  // element blocks (stencil without the pattern table)
+  __shared__ __align__(16) T sKeT[(STENCIL && !PT) ? SP_KB_SIZE : 4];
   extern __shared__ __align__(16) float s_ptab[];  // SP_PT_BYTES when PT
   __shared__ double sD[72], sBbar[144], sdsh[192];
   // block_sum<NV> needs 33*NV doubles; NV is at most max(2K, 12) <= 16
@@ -108,8 +105,6 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
   double *u = P.ws_u + (size_t)slot * P.ws_stride;
   T *ws = reinterpret_cast<T *>(P.ws_v) + (size_t)slot * 4 * P.ws_stride;
   T *r = ws, *x = ws + P.ws_stride, *p = ws + 2 * P.ws_stride, *q = ws + 3 * P.ws_stride;
-  T *vrm = reinterpret_cast<T *>(P.ws_rm) + (size_t)slot * P.rm_stride;
-  T *drm = reinterpret_cast<T *>(P.ws_drm) + (size_t)slot * P.drm_stride;
 
   for (;;) {
     // rank 0 claims the next RVE and hands it to the cluster
@@ -160,20 +155,9 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     } else {
       nsv = reinterpret_cast<T *>(P.nsv) + rv.nsv_off;
       dinv = reinterpret_cast<T *>(P.dinv) + rv.dinv_off;
-      for (int i = t; i < 2 * SP_KE; i += NT) sKeT[i] = (T)sKe[i];
-      // 2. assembly: coloured scatter into the row-major scratch, Dirichlet
-      //    rows/columns, then the node-sliced copy the solve reads
-      ell_zero<T>(gt, GNT, vrm, g.ndof);
-      rve_sync<CL>();
-      for (int c = 0; c < 8; c++) {
-        if (pl.color_off[c + 1] > pl.color_off[c])
-          scatter_colour<T>(gt, GNT, g, pl.color_elems, pl.color_off[c], pl.color_off[c + 1],
-                            pl.slot, etype, sKeT, vrm);
-        rve_sync<CL>();
-      }
-      bc_and_dinv<T>(gt, GNT, g, pl.cols, vrm, drm);
-      rve_sync<CL>();
-      ns_from_rows<T>(gt, GNT, g, pl.cols, vrm, drm, nsv, dinv);
+      // 2. assembly: every node-sliced block summed by its owner thread from
+      //    the element matrices (FP64, one rounding), Dirichlet applied
+      ns_from_elements<T>(gt, GNT, g, pl.cols, pl.nbr, etype, sKe, nsv, dinv);
     }
     if constexpr (PER) {
       // load cases: the fluctuation starts at 0; eps enters residual and averages

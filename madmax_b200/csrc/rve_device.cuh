@@ -652,6 +652,78 @@ __host__ __device__ constexpr int hex8_local(int cx, int cy, int cz) {
   return cz * 4 + (cy == 0 ? (cx ? 1 : 0) : (cx ? 2 : 3));
 }
 
+// The node-sliced values of the assembled, Dirichlet-reduced matrix straight
+// from the element matrices, without a row-major scratch or a scatter: the
+// block (node a, group m) is owned by one thread, which sums, in FP64, the
+// (a, b) blocks Ke[t][3la+d][3lb+c] of the elements holding a and its
+// neighbour b = nbr(a, m), and rounds once to T.  Dirichlet rows are
+// identity rows and Dirichlet columns zero, as bc_and_dinv leaves them;
+// unused groups (cols < 0) are zero.  The same matrix as the coloured scatter
+// followed by ns_from_rows, up to the rounding of the sums.  dinv: the
+// component-major Jacobi diagonal (1 on Dirichlet rows, 0 on padding).
+template <typename T>
+__device__ inline void ns_from_elements(int t, int nt, const MeshGeo &g,
+                                        const int *__restrict__ cols, const int *__restrict__ nbr,
+                                        const uint8_t *__restrict__ etype,
+                                        const double *Ke /*[2][576], shared*/, T *nsv, T *dinv) {
+  const size_t total = (size_t)(g.nn_pad / 32) * 27 * 32;
+  const int esy = g.nex, esz = g.nex * g.ney;
+  for (size_t x = t; x < total; x += nt) {
+    const int l = (int)(x % 32);
+    const size_t sm = x / 32;
+    const int m = (int)(sm % 27), s = (int)(sm / 27);
+    const int a = s * 32 + l;
+    double bv[9];
+#pragma unroll
+    for (int i = 0; i < 9; i++) bv[i] = 0.0;
+    if (a < g.nn && cols[(size_t)(3 * a) * SP_WP + 3 * m] >= 0) {
+      const int b = nbr[x];
+      if (is_bnode(g, a)) {
+        if (b == a) bv[0] = bv[4] = bv[8] = 1.0;
+      } else if (!is_bnode(g, b)) {
+        const int ia = a % g.nx, ja = (a / g.nx) % g.ny, ka = a / (g.nx * g.ny);
+        const int dx = b % g.nx - ia, dy = (b / g.nx) % g.ny - ja, dz = b / (g.nx * g.ny) - ka;
+        for (int c8 = 0; c8 < 8; c8++) {
+          const int ox = c8 & 1, oy = (c8 >> 1) & 1, oz = c8 >> 2;
+          const int bx = 1 - ox + dx, by = 1 - oy + dy, bz = 1 - oz + dz;
+          if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+          const int e = (ia - 1 + ox) + (ja - 1 + oy) * esy + (ka - 1 + oz) * esz;
+          const double *ke = Ke + (int)__ldg(etype + e) * SP_KE;
+          const int la = hex8_local(1 - ox, 1 - oy, 1 - oz), lb = hex8_local(bx, by, bz);
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) bv[3 * d + c] += ke[(3 * la + d) * SP_NC + 3 * lb + c];
+        }
+      }
+    }
+    T *dst = nsv + (size_t)(s * 27 + m) * 9 * 32 + l;
+#pragma unroll
+    for (int i = 0; i < 9; i++) dst[i * 32] = (T)bv[i];
+  }
+  for (int x = t; x < 3 * g.nn_pad; x += nt) {
+    const int d = x / g.nn_pad, a = x % g.nn_pad;
+    T v = T(0);
+    if (a < g.nn) {
+      if (is_bnode(g, a)) {
+        v = T(1);
+      } else {
+        const int ia = a % g.nx, ja = (a / g.nx) % g.ny, ka = a / (g.nx * g.ny);
+        double sdiag = 0.0;
+        for (int c8 = 0; c8 < 8; c8++) {
+          const int ox = c8 & 1, oy = (c8 >> 1) & 1, oz = c8 >> 2;
+          const int e = (ia - 1 + ox) + (ja - 1 + oy) * esy + (ka - 1 + oz) * esz;
+          const int la = hex8_local(1 - ox, 1 - oy, 1 - oz);
+          sdiag += Ke[(int)__ldg(etype + e) * SP_KE + (3 * la + d) * SP_NC + 3 * la + d];
+        }
+        v = (T)(1.0 / sdiag);
+      }
+    }
+    dinv[x] = v;
+  }
+}
+
+
 constexpr int SP_KB_BLK = 12;                        // padded 3x3 block (16-byte rows for float)
 // element blocks of one material, padded by 4 entries: the two materials'
 // blocks then start in different shared-memory banks, so a warp whose lanes
