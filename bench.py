@@ -68,7 +68,8 @@ def algorithmic_bytes(sizes, inner_its, outer_its, k=6, stencil=True):
     passes.  Per refinement step 3 FP64 vector passes, plus one for the
     residual of the boundary values alone (the right-hand side the stopping
     rule is relative to; the solve starts from the affine field).  Once per
-    RVE the assembled values (written) or the stencil's Jacobi diagonal."""
+    RVE the node-sliced values written (assembled operator) or the stencil's
+    Jacobi diagonal."""
     total = 0.0
     for n, it, ot in zip(sizes, inner_its, outer_its):
         n, it, ot = int(n), float(it), float(ot)
@@ -79,7 +80,7 @@ def algorithmic_bytes(sizes, inner_its, outer_its, k=6, stencil=True):
             setup = ndof * 4
         else:
             spmm = nnz_true(n) * 4 + nnz_true(n) // 9 * 4 + 2 * k * ndof * 4
-            setup = nelm * (576 * 4 + 24 * 4)
+            setup = ((n + 1) ** 3 + 31) // 32 * 32 * 243 * 4  # node-sliced values written
         vec = 8 * k * ndof * 4
         refine = 3 * k * ndof * 8
         total += it * (spmm + vec) + (ot + 2) * refine + setup
