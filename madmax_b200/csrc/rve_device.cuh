@@ -1090,8 +1090,9 @@ __device__ __forceinline__ int sp_pt_index(unsigned mask, int dx, int dy, int dz
 // it by the material pattern of the elements it shares with each neighbour.
 template <int K>
 __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const float *KB,
-                                       const uint8_t *__restrict__ etype, const float *x,
-                                       float *y, double *dot, unsigned amask, bool rev) {
+                                       const uint8_t *__restrict__ etype,
+                                       const float *__restrict__ x, float *__restrict__ y,
+                                       double *dot, unsigned amask, bool rev) {
   constexpr int KP = (K + 1) / 2;
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;

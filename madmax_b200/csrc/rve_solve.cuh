@@ -189,6 +189,75 @@ struct V16 {
   }
 };
 
+// The two FP32 vector passes of a CG step, on 16-byte chunks in node order
+// (chunk c at offset cm(c) + k*blk of load case k in the component-major
+// vectors, pb(c) + k*pk in the operator's input p).  The vectors are
+// distinct arrays (restrict-qualified), so the loads of every load case of a
+// chunk may be issued before any of its stores.
+//
+// p = D^-1 r + beta p for the load cases in am; beta 0 starts afresh from
+// D^-1 r without reading p (the work space may hold anything).
+template <typename T, int K, typename W, typename CM, typename PB>
+__device__ __forceinline__ void pass_dir(int gt, int gnt, int nch, bool rev, unsigned am,
+                                         const T *be, size_t blk, size_t pk, CM cm, PB pb,
+                                         const T *__restrict__ dinv, const T *__restrict__ r,
+                                         T *__restrict__ p) {
+  constexpr int E = W::E;
+  for (int c0 = gt; c0 < nch; c0 += gnt) {
+    const int c = rev ? nch - 1 - c0 : c0;
+    const size_t oc = cm(c), op_ = pb(c);
+    const W dv = W::load(dinv + oc);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (!((am >> k) & 1u)) continue;
+      const size_t o = (size_t)k * blk + oc, opk = op_ + k * pk;
+      const W rv = W::load(r + o);
+      W pv;
+      if (be[k] == T(0)) {
+#pragma unroll
+        for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e];
+      } else {
+        pv = W::load(p + opk);
+#pragma unroll
+        for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be[k] * pv.v[e];
+      }
+      pv.store(p + opk);
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q for the load cases in am; adds r.z and r.r
+// (z = D^-1 r) per load case into m2[k] and m2[K + k].
+template <typename T, int K, typename W, typename CM, typename PB>
+__device__ __forceinline__ void pass_xr(int gt, int gnt, int nch, bool rev, unsigned am,
+                                        const T *al, size_t blk, size_t pk, CM cm, PB pb,
+                                        const T *__restrict__ dinv, T *__restrict__ x,
+                                        const T *__restrict__ p, T *__restrict__ r,
+                                        const T *__restrict__ q, double *m2) {
+  constexpr int E = W::E;
+  for (int c0 = gt; c0 < nch; c0 += gnt) {
+    const int c = rev ? nch - 1 - c0 : c0;
+    const size_t oc = cm(c), op_ = pb(c);
+    const W dv = W::load(dinv + oc);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      if (!((am >> k) & 1u)) continue;
+      const size_t o = (size_t)k * blk + oc;
+      W xv = W::load(x + o), pv = W::load(p + op_ + k * pk), rv = W::load(r + o),
+        qv = W::load(q + o);
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        xv.v[e] += al[k] * pv.v[e];
+        rv.v[e] -= al[k] * qv.v[e];
+        m2[k] += (double)rv.v[e] * (double)(dv.v[e] * rv.v[e]);
+        m2[K + k] += (double)rv.v[e] * (double)rv.v[e];
+      }
+      xv.store(x + o);
+      rv.store(r + o);
+    }
+  }
+}
+
 // On entry u holds the start iterate with the boundary values of every load
 // case (visible to the whole cluster).  On exit avg[q*12 + 0..5] =
 // <strain>_q, avg[q*12 + 6..11] = <stress>_q (q < nrhs, shared memory of
@@ -277,27 +346,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
 #pragma unroll
     for (int k = 0; k < K; k++) be[k] = (T)sh->beta[k];
     const bool rev = (npass++ & 1) != 0;
-    for (int c0 = gt; c0 < nch; c0 += GNT) {
-      const int c = rev ? nch - 1 - c0 : c0;
-      const size_t oc = cm(c), op_ = pb(c);
-      const W dv = W::load(dinv + oc);
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        if (!((am >> k) & 1u)) continue;
-        const size_t o = (size_t)k * blk + oc, opk = op_ + k * pk;
-        const W rv = W::load(r + o);
-        W pv;
-        if (be[k] == T(0)) {  // a fresh start never reads p (the work space may hold anything)
-#pragma unroll
-          for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e];
-        } else {
-          pv = W::load(p + opk);
-#pragma unroll
-          for (int e = 0; e < E; e++) pv.v[e] = dv.v[e] * rv.v[e] + be[k] * pv.v[e];
-        }
-        pv.store(p + opk);
-      }
-    }
+    pass_dir<T, K, W>(gt, GNT, nch, rev, am, be, blk, pk, cm, pb, dinv, r, p);
   };
   for (;;) {
     // 3a. FP64 residual b = -K u -> r (type T) and its norms; on a cold
@@ -438,27 +487,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
         for (int k = 0; k < K; k++) al[k] = (T)sh->alpha[k];
         const unsigned am = sh->amask;  // converged load cases are left as they are
         const bool rev = (npass++ & 1) != 0;
-        for (int c0 = gt; c0 < nch; c0 += GNT) {
-          const int c = rev ? nch - 1 - c0 : c0;
-          const size_t oc = cm(c), op_ = pb(c);
-          const W dv = W::load(dinv + oc);
-#pragma unroll
-          for (int k = 0; k < K; k++) {
-            if (!((am >> k) & 1u)) continue;
-            const size_t o = (size_t)k * blk + oc;
-            W xv = W::load(x + o), pv = W::load(p + op_ + k * pk), rv = W::load(r + o),
-              qv = W::load(q + o);
-#pragma unroll
-            for (int e = 0; e < E; e++) {
-              xv.v[e] += al[k] * pv.v[e];
-              rv.v[e] -= al[k] * qv.v[e];
-              m2[k] += (double)rv.v[e] * (double)(dv.v[e] * rv.v[e]);
-              m2[K + k] += (double)rv.v[e] * (double)rv.v[e];
-            }
-            xv.store(x + o);
-            rv.store(r + o);
-          }
-        }
+        pass_xr<T, K, W>(gt, GNT, nch, rev, am, al, blk, pk, cm, pb, dinv, x, p, r, q, m2);
         rve_reduce<2 * K, CL>(m2, red, sh);
         if (warp == 0) {
           bool a = false;
