@@ -114,7 +114,7 @@ PROFILED_TRAFFIC = {
     # dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
     # -k regex:k_batch -s 13 -c 1 python bench.py --steps 1 --warmup 3 ...
     "k_batch --nrve 4096 --sizes 8 12 16 20 --op stencil --threads 0 --ctas 0 "
-    "--inner-rtol 0.0001": 686171300096,
+    "--inner-rtol 0.003": 649592013568,
     # k_spmv_rve, the n = 40 structured matrix, cold L2
     "k_spmv_rve structured ELL n=40": 214213376,
 }
@@ -830,7 +830,8 @@ def main(argv=None):
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0: the library's choice)")
     ap.add_argument("--ctas", type=int, default=0, help="CTAs per SM (0: the library's choice)")
     ap.add_argument("--cluster", type=int, default=1)
-    ap.add_argument("--inner-rtol", type=float, default=1e-4)
+    ap.add_argument("--inner-rtol", type=float, default=3e-3,
+                    help="CG residual reduction per refinement step (the library's default)")
     ap.add_argument("--op", default="stencil", choices=["stencil", "ell"],
                     help="inner CG operator: element-type stencil or assembled ELL values")
     ap.add_argument("--sizes", type=int, nargs="+", default=list(SIZES),

@@ -339,9 +339,7 @@ static int rve_solve_k(sp_rve *r, Device *d, PcgGraph<double, K, 32> *&pcg, int 
     if (done || outer >= max_outer) break;
     PcgState st0 = {};
     st0.nactive = nrhs;
-    // each correction to a quarter of the target (the margin of the batch's
-    // corrections, rve_solve.cuh)
-    st0.rtol2 = (0.25 * rtol) * (0.25 * rtol);
+    st0.rtol2 = (0.5 * rtol) * (0.5 * rtol);
     st0.max_its = 20000;
     SP_CUDA_TRY(cudaMemcpyAsync(r->d_st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
     int fixed = 0;

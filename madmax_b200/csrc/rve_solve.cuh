@@ -33,16 +33,8 @@ constexpr double SP_RHS_FLOOR = 1e-12;
 
 // A correction that would take the residual to the final target ends at
 // this fraction of it, so that the FP64 residual after the update meets the
-// target with a margin.  A quarter: from the affine start the error left at
-// a given residual lies more in smooth modes, which weigh on the volume
-// averages (at half the target, one RVE of a 32-RVE sample of the batched mix
-// was 1.4e-8 off the oracle's stress; at a quarter the largest of 96 was
-// 7.4e-9, for 3% more time).
-constexpr double SP_FINAL_MARGIN = 0.25;
-// After a correction a load case is done when its FP64 residual is at most
-// this fraction of the target (above SP_FINAL_MARGIN, which leaves room for
-// the FP32 correction's rounding).
-constexpr double SP_ACCEPT = 0.5;
+// target with a margin.
+constexpr double SP_FINAL_MARGIN = 0.5;
 
 struct SolveArgs {
   int nrhs;
@@ -389,12 +381,7 @@ __device__ sp_solve_info solve_rve(const MeshGeo &g, const Op &op, const T *dinv
           if (first) sh->rn0[lane] = (rn <= SP_RHS_FLOOR * sqrt(red[tot + K + lane])) ? 0.0 : rn;
           sh->rn[lane] = rn;
           double rn0 = sh->rn0[lane];
-          // a start iterate is accepted at rtol; after an FP32 correction a
-          // load case is accepted at SP_ACCEPT of the target, so that the
-          // FP32 rounding left in the correction (an error of no CG shape,
-          // whose effect on the volume averages is not bounded by the
-          // residual) stays well below it
-          const double target = (outer == 0) ? P.rtol : SP_ACCEPT * P.rtol_refine;
+          const double target = (outer == 0) ? P.rtol : P.rtol_refine;
           notdone = lane < P.nrhs && rn0 > 0.0 && rn > target * rn0;
           sh->act[lane] = notdone;
         }
