@@ -203,9 +203,10 @@ typedef struct {
   int nrhs;          /* load cases per RVE, 1..8 (default 6) */
   int precision;     /* SP_PREC_MIXED (default) or SP_PREC_FP64 */
   double rtol;       /* FP64 residual target per rhs (default 1e-8) */
-  double inner_rtol; /* CG residual reduction per refinement step (default 3e-3: short
-                        corrections, each replaced by the FP64 residual, keep the FP32
-                        rounding in the volume averages small) */
+  double inner_rtol; /* CG residual reduction per refinement step (0: 3e-3 in mixed
+                        precision -- short FP32 corrections, each replaced by the FP64
+                        residual, keep the rounding in the volume averages small --
+                        and 1e-4 in FP64) */
   int max_outer;     /* refinement steps (default 8) */
   int max_inner;     /* CG iterations per step (default 4000) */
   int threads;       /* threads per CTA: 256, 512, 1024 (0: chosen, see tune) */

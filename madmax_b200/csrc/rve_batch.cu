@@ -297,7 +297,7 @@ extern "C" void sp_batch_opts_default(sp_batch_opts *o) {
   o->nrhs = 6;
   o->precision = SP_PREC_MIXED;
   o->rtol = 1e-8;
-  o->inner_rtol = 3e-3;
+  o->inner_rtol = 0.0;  // chosen by precision at create time
   o->max_outer = 8;
   o->max_inner = 4000;
   o->threads = 0;      // chosen per operator at create time
@@ -367,7 +367,9 @@ extern "C" int sp_batch_create(int nrve, const sp_rve_desc *descs, const sp_batc
   if (o.max_outer < 1) o.max_outer = 8;
   if (o.max_inner < 1) o.max_inner = 4000;
   if (!(o.rtol > 0)) o.rtol = 1e-8;
-  if (!(o.inner_rtol > 0)) o.inner_rtol = 3e-3;
+  // FP32 corrections of 3e-3, each replaced by the FP64 residual, keep the
+  // rounding in the volume averages small; FP64 corrections can run longer
+  if (!(o.inner_rtol > 0)) o.inner_rtol = (o.precision == SP_PREC_FP64) ? 1e-4 : 3e-3;
   for (int i = 0; i < nrve; i++)
     for (int k = 0; k < 3; k++) {
       if (descs[i].n[k] < 1 || descs[i].len[k] <= 0)
