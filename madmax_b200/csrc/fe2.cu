@@ -17,7 +17,8 @@
 //   4. Jacobian K = sum_e sum_gp B^T C B w (macro/src/assembly.c:165-222)
 //      into FP64 ELL by the 8-colour conflict-free scatter, clamped rows and
 //      columns set to the identity (MatZeroRowsColumns, :208-214);
-//   5. K dx = b by the graph-captured FP64 Jacobi-PCG (pcg.cuh), u += dx.
+//   5. K dx = b by the FP64 Jacobi-PCG in one cooperative launch (pcg.cuh,
+//      k_pcg_coop), u += dx.
 // The iteration stops after newton_its, or when ||b|| <= newton_tol (the
 // reference's check before assembling, macro/src/main.c:222-227).
 #include <time.h>
@@ -222,7 +223,7 @@ struct sp_fe2_s {
   PcgState *d_st = nullptr;
   double *d_partial = nullptr;
   unsigned *d_ticket = nullptr;
-  PcgGraph<double, 1, 8> *pcg = nullptr;
+  PcgCoop<double, 1, 8> *pcg = nullptr;
   int nblk = 0;
   cudaStream_t stream = nullptr;
 };
@@ -352,11 +353,16 @@ extern "C" int sp_fe2_create(const sp_fe2_desc *desc, sp_fe2 **out) {
   }
   if (!rc && D.micro == SP_FE2_LINEAR) rc = fe2_linear_tangents(f);
   if (!rc) {
-    f->nblk = (int)std::min<long long>(4096, std::max<long long>(1, ((long long)nd * 8 / 32 + 7) / 8));
-    f->pcg = new PcgGraph<double, 1, 8>();
+    // the macro system (14,883 dof for 40x10x10) is small: one cooperative
+    // launch per solve instead of three launches per CG iteration
+    f->pcg = new PcgCoop<double, 1, 8>();
     double *vr = f->d_vec, *vp = vr + nd, *vq = vp + nd, *vdx = vq + nd;
-    rc = f->pcg->build(f->stream, f->nblk, (int)nd, SP_WP, f->d_vals, f->plan->cols, f->d_dinv,
-                       f->d_b, vdx, vr, vp, vq, 1, f->d_st, f->d_partial, f->d_ticket);
+    Device *dv;
+    rc = device(&dv);
+    if (!rc)
+      rc = f->pcg->build(dv, 2048, (int)nd, SP_WP, f->d_vals, f->plan->cols, f->d_dinv, f->d_b,
+                         vdx, vr, vp, vq, f->d_st, f->d_partial);
+    if (!rc) f->nblk = f->pcg->nblk;
   }
   if (rc) {
     sp_fe2_destroy(f);
@@ -452,7 +458,7 @@ extern "C" int sp_fe2_run(sp_fe2 *f, sp_fe2_info *info) {
     st0.rtol2 = f->d.lin_rtol * f->d.lin_rtol;
     st0.max_its = 100000;
     SP_CUDA_TRY(cudaMemcpyAsync(f->d_st, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
-    SP_TRY(f->pcg->run(s, nullptr));
+    SP_TRY(f->pcg->run(s));
     k_fe2_axpy<<<blocks(nd), 256, 0, s>>>((int)nd, vdx, f->d_u);
     SP_CUDA_TRY(cudaGetLastError());
     SP_CUDA_TRY(cudaEventRecord(ev[3], s));

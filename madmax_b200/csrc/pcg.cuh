@@ -12,6 +12,10 @@
 // every right-hand side has converged or the iteration limit is reached.
 #pragma once
 
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "sp_cuda.h"
 
 namespace sp {
@@ -271,6 +275,182 @@ struct PcgGraph {
     graph = nullptr;
   }
   ~PcgGraph() { destroy(); }
+};
+
+// The whole Jacobi-PCG (x0 = 0) in one cooperative launch, for matrices
+// small enough that the three launches of an iteration cost more than their
+// work.  Grid barriers separate the phases; a phase's per-block partial sums
+// go to one of two partial arrays (two barriers lie between a block's read
+// of an array and the next write to it), and every block folds the partials
+// in the same order, so all blocks hold identical scalars without a
+// broadcast and take the same exit: every right-hand side converged or
+// st->max_its reached.  The vector reads of p are coherent: the kernel writes
+// p itself.  Block 0 leaves the final state in st, as the graph solve does.
+template <typename T, int K, int L>
+__global__ void __launch_bounds__(PCG_THREADS)
+    k_pcg_coop(int n, int wp, const T *__restrict__ vals, const int *__restrict__ cols,
+               const T *__restrict__ dinv, const T *__restrict__ b, T *x, T *r, T *p, T *q,
+               PcgState *st, double *part_a, double *part_b) {
+  namespace cgr = cooperative_groups;
+  cgr::grid_group grid = cgr::this_grid();
+  __shared__ double red[33 * 2 * K];
+  __shared__ double tot[2 * K];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+  const int nb = gridDim.x;
+  // every block folds the partials of `part` (NV per block) in block order
+  auto fold = [&](const double *part, int nv, double *out) {
+    double acc[2 * K];
+    #pragma unroll
+    for (int v = 0; v < 2 * K; v++) acc[v] = 0.0;
+    for (int blk = threadIdx.x; blk < nb; blk += blockDim.x)
+      for (int v = 0; v < nv; v++) acc[v] += __ldcg(part + blk * nv + v);
+    block_sum<2 * K>(acc, red, out);
+  };
+  auto publish = [&](const double *mine, double *part, int nv) {
+    double bs[2 * K];
+    block_sum<2 * K>(mine, red, bs);
+    if (threadIdx.x == 0)
+      for (int v = 0; v < nv; v++) part[blockIdx.x * nv + v] = bs[v];
+  };
+  const double rtol2 = st->rtol2;
+  const int max_its = st->max_its, nrhs = st->nactive;
+  // start: x = 0, r = b, p = z = D^-1 b; rho = r.z, bb = b.b
+  double mine[2 * K];
+  #pragma unroll
+  for (int v = 0; v < 2 * K; v++) mine[v] = 0.0;
+  for (int i = t; i < n; i += nt) {
+    const T di = dinv[i];
+    #pragma unroll
+    for (int k = 0; k < K; k++) {
+      const size_t o = (size_t)i * K + k;
+      const T bv = b[o];
+      x[o] = 0;
+      r[o] = bv;
+      const T z = di * bv;
+      p[o] = z;
+      mine[k] += (double)bv * (double)z;
+      mine[K + k] += (double)bv * (double)bv;
+    }
+  }
+  publish(mine, part_b, 2 * K);
+  grid.sync();
+  double rho[K], bb[K], rr[K], alpha[K], beta[K];
+  int act[K];
+  fold(part_b, 2 * K, tot);
+  int na = 0;
+  #pragma unroll
+  for (int k = 0; k < K; k++) {
+    rho[k] = tot[k];
+    bb[k] = tot[K + k];
+    rr[k] = bb[k];
+    alpha[k] = beta[k] = 0.0;
+    act[k] = bb[k] > 0.0 && k < nrhs;
+    na += act[k];
+  }
+  int its = 0;
+  while (na > 0 && its < max_its) {
+    // q = A p, alpha = rho / p.q
+    double pq[2 * K];
+    #pragma unroll
+    for (int v = 0; v < 2 * K; v++) pq[v] = 0.0;
+    spmm<T, K, L, false>(t, nt, n, wp, vals, cols, p, q, pq);
+    publish(pq, part_a, K);
+    grid.sync();
+    fold(part_a, K, tot);
+    #pragma unroll
+    for (int k = 0; k < K; k++) alpha[k] = (act[k] && tot[k] != 0.0) ? rho[k] / tot[k] : 0.0;
+    // x += alpha p, r -= alpha q; r.z, r.r
+    #pragma unroll
+    for (int v = 0; v < 2 * K; v++) mine[v] = 0.0;
+    for (int i = t; i < n; i += nt) {
+      const T di = dinv[i];
+      #pragma unroll
+      for (int k = 0; k < K; k++) {
+        const size_t o = (size_t)i * K + k;
+        x[o] += (T)alpha[k] * p[o];
+        const T rv = r[o] - (T)alpha[k] * q[o];
+        r[o] = rv;
+        mine[k] += (double)rv * (double)(di * rv);
+        mine[K + k] += (double)rv * (double)rv;
+      }
+    }
+    publish(mine, part_b, 2 * K);
+    grid.sync();
+    fold(part_b, 2 * K, tot);
+    na = 0;
+    #pragma unroll
+    for (int k = 0; k < K; k++) {
+      rr[k] = tot[K + k];
+      if (act[k] && rr[k] <= rtol2 * bb[k]) act[k] = 0;
+      beta[k] = (act[k] && rho[k] != 0.0) ? tot[k] / rho[k] : 0.0;
+      if (act[k]) rho[k] = tot[k];
+      na += act[k];
+    }
+    its++;
+    if (na == 0 || its >= max_its) break;
+    // p = D^-1 r + beta p
+    for (int i = t; i < n; i += nt) {
+      const T di = dinv[i];
+      #pragma unroll
+      for (int k = 0; k < K; k++) {
+        const size_t o = (size_t)i * K + k;
+        p[o] = di * r[o] + (T)beta[k] * p[o];
+      }
+    }
+    grid.sync();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    #pragma unroll
+    for (int k = 0; k < K; k++) {
+      st->rho[k] = rho[k];
+      st->bb[k] = bb[k];
+      st->rr[k] = rr[k];
+      st->alpha[k] = alpha[k];
+      st->beta[k] = beta[k];
+      st->active[k] = act[k];
+    }
+    st->its = its;
+    st->nactive = na;
+  }
+}
+
+// A cooperative Jacobi-PCG solve of A x = b from x = 0 (k_pcg_coop): one
+// launch per solve, as many blocks as can be resident at once (at most what
+// the rows need).  The caller writes st->nactive (= number of rhs),
+// st->rtol2 and st->max_its before run(); partial holds 2 x 2K doubles per
+// block.
+template <typename T, int K, int L>
+struct PcgCoop {
+  int nblk = 0, n = 0, wp = 0;
+  const T *vals = nullptr, *dinv = nullptr, *b = nullptr;
+  const int *cols = nullptr;
+  T *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr;
+  PcgState *st = nullptr;
+  double *partial = nullptr;
+
+  int build(const Device *d, int max_blk, int n_, int wp_, const T *vals_, const int *cols_,
+            const T *dinv_, const T *b_, T *x_, T *r_, T *p_, T *q_, PcgState *st_,
+            double *partial_) {
+    n = n_; wp = wp_; vals = vals_; cols = cols_; dinv = dinv_; b = b_;
+    x = x_; r = r_; p = p_; q = q_; st = st_; partial = partial_;
+    int occ = 0;
+    SP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_coop<T, K, L>,
+                                                              PCG_THREADS, 0));
+    if (occ < 1) return sp_set_error(SP_ERR_CUDA, "cooperative PCG: no block fits an SM");
+    const long long need = ((long long)n * L + PCG_THREADS - 1) / PCG_THREADS;
+    nblk = (int)std::min<long long>(std::min<long long>(need, (long long)d->nsm * occ), max_blk);
+    if (nblk < 1) nblk = 1;
+    return SP_OK;
+  }
+  int run(cudaStream_t s) {
+    double *pa = partial, *pb = partial + (size_t)nblk * 2 * K;
+    void *args[] = {(void *)&n, (void *)&wp, (void *)&vals, (void *)&cols, (void *)&dinv,
+                    (void *)&b, (void *)&x, (void *)&r, (void *)&p, (void *)&q,
+                    (void *)&st, (void *)&pa, (void *)&pb};
+    SP_CUDA_TRY(cudaLaunchCooperativeKernel((const void *)k_pcg_coop<T, K, L>, dim3(nblk),
+                                            dim3(PCG_THREADS), args, 0, s));
+    return SP_OK;
+  }
 };
 
 }  // namespace sp
