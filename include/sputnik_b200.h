@@ -204,9 +204,10 @@ typedef struct {
   int precision;     /* SP_PREC_MIXED (default) or SP_PREC_FP64 */
   double rtol;       /* FP64 residual target per rhs (default 1e-8) */
   double inner_rtol; /* CG residual reduction per refinement step (0: 3e-3 in mixed
-                        precision -- short FP32 corrections, each replaced by the FP64
-                        residual, keep the rounding in the volume averages small --
-                        and 1e-4 in FP64) */
+                        precision under affine conditions -- short FP32 corrections,
+                        each replaced by the FP64 residual, keep the rounding in the
+                        volume averages small -- and 1e-4 in FP64 or under periodic
+                        conditions) */
   int max_outer;     /* refinement steps (default 8) */
   int max_inner;     /* CG iterations per step (default 4000) */
   int threads;       /* threads per CTA: 256, 512, 1024 (0: chosen, see tune) */

@@ -17,7 +17,7 @@ constexpr int SP_OP_STENCIL_PER = 2;
 // which it keeps in SP_PT_BYTES of dynamic shared memory; more than 6 load
 // cases need the wide register budget
 __host__ __device__ constexpr bool sp_batch_uses_ptable(bool fp32, int K, int op, bool wide = false) {
-  return op == SP_OP_STENCIL && fp32 && (K <= 6 || wide);
+  return (op == SP_OP_STENCIL || op == SP_OP_STENCIL_PER) && fp32 && (K <= 6 || wide);
 }
 
 // Dynamic shared memory of a k_batch variant: the pattern table or nothing.

@@ -790,6 +790,25 @@ constexpr int SP_PT_REC = 12;              // floats per block (9 + 3 pads: 16-b
 constexpr int SP_PT_BYTES = SP_PT_NREC * SP_PT_REC * 4;
 static_assert(SP_PT_NREC == 256 + 6 * 16 + 12 * 4 + 8 * 2, "pattern table size");
 
+// The pattern-table block of a node with material mask `mask` (bit c: the
+// element at corner c) for the neighbour at offset (dx, dy, dz).
+__device__ __forceinline__ int sp_pt_index(unsigned mask, int dx, int dy, int dz) {
+  unsigned q0 = 0, q1 = 0;
+  int nb = 0;
+#pragma unroll
+  for (int c2 = 0; c2 < 4; c2++) {
+    const int ox = c2 & 1, oy = c2 >> 1;
+    if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
+    q0 |= ((mask >> c2) & 1u) << nb;
+    q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
+    nb++;
+  }
+  const int m0 = (dx + 1) + 3 * (dy + 1);
+  return dz < 0 ? sp_pt_off(m0) + (int)q0
+                : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb)) : sp_pt_off(m0 + 18) + (int)q1);
+}
+
+
 // Bytes of dynamic shared memory the running kernel was launched with.  A
 // kernel that keeps the pattern table there checks it first: a launch
 // without it would read and write past the block's shared memory.
@@ -949,8 +968,10 @@ struct StencilAcc<double, K> {
 // from the element blocks of their own materials.  Adds x.y per load case
 // into dot[K].  Load cases whose bit in amask is clear (converged; uniform
 // across the block) are neither read nor written.  rev: the warps walk the
-// node groups from the last to the first.
-template <typename T, int K, bool PER = false>
+// node groups from the last to the first.  PT: KB is the FP32 pattern table
+// (stencil_ptable) and every lane reads each of its 27 blocks from it by the
+// material pattern of the (wrapped) elements it shares with the neighbour.
+template <typename T, int K, bool PER = false, bool PT = false>
 __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB,
                                     const uint8_t *__restrict__ etype, const T *x, T *y,
                                     double *dot, unsigned amask = ~0u, bool rev = false) {
@@ -1006,7 +1027,18 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
     acc.zero();
     const bool all0 = __all_sync(0xffffffffu, mask == 0u);
     const bool all1 = __all_sync(0xffffffffu, mask == 0xffu);
-    if (all0 || all1) {
+    if constexpr (PT) {
+#pragma unroll 1
+      for (int dz = -1; dz <= 1; dz++) {
+#pragma unroll
+        for (int mm = 0; mm < 9; mm++) {
+          const int dx = mm % 3 - 1, dy = mm / 3 - 1;
+          A bv[9] = {};
+          add_block<T, A>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
+          acc.fma_block(bv, x + nbk_base<K>(nbr_of(dx, dy, dz)), amask);
+        }
+      }
+    } else if (all0 || all1) {
       // one material around every node of the warp: its assembled blocks
       const T *ka = KB + SP_KA_OFF + (all1 ? 27 * SP_KB_BLK : 0);
 #pragma unroll 1
@@ -1057,24 +1089,6 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
       }
     }
   }
-}
-
-// The pattern-table block of a node with material mask `mask` (bit c: the
-// element at corner c) for the neighbour at offset (dx, dy, dz).
-__device__ __forceinline__ int sp_pt_index(unsigned mask, int dx, int dy, int dz) {
-  unsigned q0 = 0, q1 = 0;
-  int nb = 0;
-#pragma unroll
-  for (int c2 = 0; c2 < 4; c2++) {
-    const int ox = c2 & 1, oy = c2 >> 1;
-    if ((dx < 0 && ox) || (dx > 0 && !ox) || (dy < 0 && oy) || (dy > 0 && !oy)) continue;
-    q0 |= ((mask >> c2) & 1u) << nb;
-    q1 |= ((mask >> (c2 + 4)) & 1u) << nb;
-    nb++;
-  }
-  const int m0 = (dx + 1) + 3 * (dy + 1);
-  return dz < 0 ? sp_pt_off(m0) + (int)q0
-                : (dz == 0 ? sp_pt_off(m0 + 9) + (int)(q0 | (q1 << nb)) : sp_pt_off(m0 + 18) + (int)q1);
 }
 
 // FP32 stencil SpMM under Dirichlet conditions with the x-neighbours taken

@@ -150,16 +150,16 @@ struct EllOp {
 
 template <typename T, int K, bool PER = false, bool PT = false>
 struct StencilOp {
-  static_assert(!PT || (sizeof(T) == 4 && !PER), "pattern tables serve the FP32 Dirichlet stencil");
+  static_assert(!PT || sizeof(T) == 4, "pattern tables serve the FP32 stencil");
   static constexpr bool kBlocked = true;  // p node-blocked (nbk_base)
   const T *kb;  // shared-memory blocks: stencil_blocks, or stencil_ptable when PT
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
                         unsigned amask, bool rev) const {
-    if constexpr (PT)
+    if constexpr (PT && !PER)
       spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
     else
-      spmm_stencil<T, K, PER>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+      spmm_stencil<T, K, PER, PT>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
   }
 };
 

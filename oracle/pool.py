@@ -55,6 +55,16 @@ def fd_tangent(item):
     return s0, Cm
 
 
+def homogenize_periodic(item):
+    """item = (n, radius, (Em, Ef), (num, nuf), strains [k,6]) -> stress [k,6]
+    under periodic conditions (oracle/periodic.py, direct solve)."""
+    from . import periodic as PER
+    n, radius, E, nu, strains = item
+    m, et = _mesh(n, radius)
+    _, st, _ = PER.homogenize_periodic(m, et, tuple(E), tuple(nu), np.asarray(strains))
+    return st
+
+
 def run(fn, items, procs: int = 0):
     """[fn(item) for item in items], largest meshes first over a spawned pool
     of `procs` processes (0: every host core, at most len(items))."""
