@@ -866,7 +866,24 @@ __device__ inline void stencil_dinv(int t, int nt, const MeshGeo &g,
   }
 }
 
-// 3x3 block load from shared memory (16-byte loads), accumulated into bv
+// 3x3 block load from shared memory (16-byte loads) into bv.  A block read
+// on its own goes through load_block, not add_block into zeros: 0 + w is not
+// w for w = -0, so the compiler keeps those 9 additions (a sixth of the FP32
+// pipe's work in the stencil SpMM).
+template <typename T, typename A>
+__device__ __forceinline__ void load_block(const T *src, A *bv) {
+  constexpr int BW = SP_KB_BLK * (int)sizeof(T) / 16;
+  T w[SP_KB_BLK];
+#pragma unroll
+  for (int q = 0; q < BW; q++) {
+    int4 v = reinterpret_cast<const int4 *>(src)[q];
+    memcpy(reinterpret_cast<char *>(w) + 16 * q, &v, 16);
+  }
+#pragma unroll
+  for (int u = 0; u < 9; u++) bv[u] = (A)w[u];
+}
+
+// the same, accumulated into bv (sums of element blocks)
 template <typename T, typename A>
 __device__ inline void add_block(const T *src, A *bv) {
   constexpr int BW = SP_KB_BLK * (int)sizeof(T) / 16;
@@ -1033,8 +1050,8 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 #pragma unroll
         for (int mm = 0; mm < 9; mm++) {
           const int dx = mm % 3 - 1, dy = mm / 3 - 1;
-          A bv[9] = {};
-          add_block<T, A>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
+          A bv[9];
+          load_block<T, A>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
           acc.fma_block(bv, x + nbk_base<K>(nbr_of(dx, dy, dz)), amask);
         }
       }
@@ -1046,8 +1063,8 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 #pragma unroll
         for (int mm = 0; mm < 9; mm++) {
           const int dx = mm % 3 - 1, dy = mm / 3 - 1;
-          A bv[9] = {};
-          add_block<T, A>(ka + ((dz + 1) * 9 + mm) * SP_KB_BLK, bv);
+          A bv[9];
+          load_block<T, A>(ka + ((dz + 1) * 9 + mm) * SP_KB_BLK, bv);
           acc.fma_block(bv, x + nbk_base<K>(nbr_of(dx, dy, dz)), amask);
         }
       }
@@ -1102,6 +1119,8 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
 // per value; the materials and output are those of spmm_stencil.  KB is
 // the pattern table (stencil_ptable): every lane reads its 27 blocks from
 // it by the material pattern of the elements it shares with each neighbour.
+// Used for K > 6 load cases, where the three accumulator sets of
+// spmm_stencil_xo do not fit in the registers.
 template <int K>
 __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const float *KB,
                                        const uint8_t *__restrict__ etype,
@@ -1163,8 +1182,8 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
       const float2 (&xv)[3][KP] = xr[r & 1];
 #pragma unroll
       for (int dx = -1; dx <= 1; dx++) {
-        float bv[9] = {};
-        add_block<float, float>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
+        float bv[9];
+        load_block<float, float>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
 #pragma unroll
         for (int p = 0; p < KP; p++) {
           if (!((amask >> (2 * p)) & 3u)) continue;
@@ -1202,6 +1221,129 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const float yv = (q & 1) ? acc[d][q >> 1].y : acc[d][q >> 1].x;
+          dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
+          y[q * blk + (size_t)d * g.nn_pad + a] = yv;
+        }
+      }
+    }
+  }
+}
+
+// FP32 stencil SpMM under Dirichlet conditions, the x-neighbour terms formed
+// where the x values already are.  A warp holds 32 consecutive interior
+// nodes: lanes 1..30 produce output, lanes 0 and 31 only contribute.  For
+// each of the 9 (dy, dz) neighbour rows a lane gathers the 3K values of its
+// own column (one gather per value instead of three) and multiplies them by
+// three blocks: its own (dx = 0), the one its right neighbour b+1 would apply
+// to them (b+1's dx = -1 block), and the one its left neighbour b-1 would
+// apply (b-1's dx = +1 block).  Those two blocks depend on the materials of
+// the elements the neighbour shares with the row, which are elements around
+// this node too: b+1's ox = 0 elements are this node's ox = 1 elements, and
+// b-1's ox = 1 elements its ox = 0 ones, so their pattern-table records are
+// found from this lane's own mask.  The two partial sums cross lanes once per
+// warp trip (36 shuffles instead of 324 for the inputs), and are added only
+// where the neighbour is an interior node of the same row (the CG vectors
+// vanish on the Dirichlet boundary).  Same blocks and products as
+// spmm_stencil; the sums differ in order only.  The shared-memory pipe that
+// serves the shuffles, the pattern-table loads and the gathers' L1 hits is
+// what bounds this operator: this form needs 31% fewer of its wavefronts.
+// KB is the pattern table (stencil_ptable).
+template <int K>
+__device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const float *KB,
+                                       const uint8_t *__restrict__ etype,
+                                       const float *__restrict__ x, float *__restrict__ y,
+                                       double *dot, unsigned amask, bool rev) {
+  constexpr int KP = (K + 1) / 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = t & 31, warp = t >> 5, nwarps = nt >> 5;
+  const int mx = g.nx - 2, my = g.ny - 2, mz = g.nz - 2;
+  const int ni = mx * my * mz;
+  const int sy = g.nx, sz = g.nx * g.ny;
+  const int esy = g.nex, esz = g.nex * g.ney;
+  const size_t blk = (size_t)3 * g.nn_pad;
+  const int ngr = (ni + 29) / 30;
+  for (int gi = warp; gi < ngr; gi += nwarps) {
+    const int s0 = (rev ? ngr - 1 - gi : gi) * 30;
+    const int id = s0 - 1 + lane;
+    const bool out = lane >= 1 && lane <= 30 && id < ni;
+    const int idc = min(max(id, 0), ni - 1);
+    const int ii = idc % mx, jj = (idc / mx) % my, kk = idc / (mx * my);
+    const int i = ii + 1, j = jj + 1, k = kk + 1;
+    const int a = i + j * sy + k * sz;
+    // the adjacent lanes hold the x-neighbours unless those are boundary nodes
+    const bool lo = ii > 0, hi = ii < mx - 1;
+    unsigned mask = 0;  // bit c: material of the element at corner c
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+      const int e = (i - 1 + ox) + (j - 1 + oy) * esy + (k - 1 + oz) * esz;
+      mask |= (unsigned)__ldg(etype + e) << c;
+    }
+    // the masks b+1 and b-1 would use, as far as their dx = -1 / +1 blocks
+    // read them (sp_pt_index reads only the ox = 0 / ox = 1 bits there)
+    const unsigned mR = (mask >> 1) & 0x55u, mL = (mask << 1) & 0xAAu;
+    float2 acc[3][3][KP];  // [own, for b+1, for b-1][d][load-case pair]
+#pragma unroll
+    for (int s = 0; s < 3; s++)
+#pragma unroll
+      for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int p = 0; p < KP; p++) acc[s][d][p] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+      const int dy = r % 3 - 1, dz = r / 3 - 1;
+      const float *xb = x + nbk_base<K>(a + dy * sy + dz * sz);
+      float2 xv[3][KP];
+#pragma unroll
+      for (int p = 0; p < KP; p++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          xv[c][p] = make_float2(0.f, 0.f);
+          if ((amask >> (2 * p)) & 3u) {
+            xv[c][p].x = xb[(c * K + 2 * p) * 32];
+            if (2 * p + 1 < K) xv[c][p].y = xb[(c * K + 2 * p + 1) * 32];
+          }
+        }
+#pragma unroll
+      for (int s = 0; s < 3; s++) {
+        const int rec = s == 0 ? sp_pt_index(mask, 0, dy, dz)
+                               : (s == 1 ? sp_pt_index(mR, -1, dy, dz) : sp_pt_index(mL, 1, dy, dz));
+        float bv[9];
+        load_block<float, float>(KB + rec * SP_PT_REC, bv);
+#pragma unroll
+        for (int p = 0; p < KP; p++) {
+          if (!((amask >> (2 * p)) & 3u)) continue;
+#pragma unroll
+          for (int d = 0; d < 3; d++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const float b = bv[d * 3 + c];
+              acc[s][d][p] = __ffma2_rn(make_float2(b, b), xv[c][p], acc[s][d][p]);
+            }
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < KP; p++) {
+      if (!((amask >> (2 * p)) & 3u)) continue;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        float2 v;
+        v.x = __shfl_up_sync(FULL, acc[1][d][p].x, 1);
+        v.y = __shfl_up_sync(FULL, acc[1][d][p].y, 1);
+        if (lo) acc[0][d][p] = make_float2(acc[0][d][p].x + v.x, acc[0][d][p].y + v.y);
+        v.x = __shfl_down_sync(FULL, acc[2][d][p].x, 1);
+        v.y = __shfl_down_sync(FULL, acc[2][d][p].y, 1);
+        if (hi) acc[0][d][p] = make_float2(acc[0][d][p].x + v.x, acc[0][d][p].y + v.y);
+      }
+    }
+    if (out) {
+#pragma unroll
+      for (int q = 0; q < K; q++) {
+        if (!((amask >> q) & 1u)) continue;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const float yv = (q & 1) ? acc[0][d][q >> 1].y : acc[0][d][q >> 1].x;
           dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
           y[q * blk + (size_t)d * g.nn_pad + a] = yv;
         }

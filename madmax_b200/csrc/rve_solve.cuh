@@ -156,7 +156,9 @@ struct StencilOp {
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
                         unsigned amask, bool rev) const {
-    if constexpr (PT && !PER)
+    if constexpr (PT && !PER && K <= 6)
+      spmm_stencil_xo<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
+    else if constexpr (PT && !PER)
       spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
     else
       spmm_stencil<T, K, PER, PT>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
