@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(BatchParams P) {
     sa.eps = seps;
     sp_solve_info in;
     if constexpr (STENCIL) {
-      StencilOp<T, K, PER, PT> op{PT ? reinterpret_cast<const T *>(s_ptab) : sKeT, etype};
+      StencilOp<T, K, PER, PT, WIDE> op{PT ? reinterpret_cast<const T *>(s_ptab) : sKeT, etype};
       in = solve_rve<T, K, NT, CL, decltype(op), WIDE>(g, op, dinv, etype, sKe, sD, sBbar, u, r,
                                                        x, p, q, sa, red, &sh, savg);
     } else {

@@ -148,7 +148,10 @@ struct EllOp {
   }
 };
 
-template <typename T, int K, bool PER = false, bool PT = false>
+// XO: the x-neighbour terms formed in the lane holding the values
+// (spmm_stencil_xo), for up to 6 load cases in kernels with 128 registers a
+// thread; its three accumulator sets spill heavily below that.
+template <typename T, int K, bool PER = false, bool PT = false, bool XO = true>
 struct StencilOp {
   static_assert(!PT || sizeof(T) == 4, "pattern tables serve the FP32 stencil");
   static constexpr bool kBlocked = true;  // p node-blocked (nbk_base)
@@ -156,7 +159,7 @@ struct StencilOp {
   const uint8_t *etype;
   __device__ void apply(int gt, int gnt, const MeshGeo &g, const T *p, T *q, double *dot,
                         unsigned amask, bool rev) const {
-    if constexpr (PT && !PER && K <= 6)
+    if constexpr (PT && !PER && K <= 6 && XO)
       spmm_stencil_xo<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
     else if constexpr (PT && !PER)
       spmm_stencil_xw<K>(gt, gnt, g, kb, etype, p, q, dot, amask, rev);
