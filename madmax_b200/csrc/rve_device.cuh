@@ -786,8 +786,10 @@ __host__ __device__ constexpr int sp_pt_off(int m) {
   return o;
 }
 constexpr int SP_PT_NREC = sp_pt_off(27);  // 416 blocks
-constexpr int SP_PT_REC = 12;              // floats per block (9 + 3 pads: 16-byte rows)
-constexpr int SP_PT_BYTES = SP_PT_NREC * SP_PT_REC * 4;
+// Layout: entries 0..7 of block b at [8b, 8b+8) (two 16-byte loads), entry 8
+// at [8 * SP_PT_NREC + b]: 36 bytes read per block and 15 KB in all, no
+// padding (records of 9 + 3 padding floats took 20 KB).
+constexpr int SP_PT_BYTES = SP_PT_NREC * 9 * 4;
 static_assert(SP_PT_NREC == 256 + 6 * 16 + 12 * 4 + 8 * 2, "pattern table size");
 
 // The pattern-table block of a node with material mask `mask` (bit c: the
@@ -818,25 +820,34 @@ __device__ inline unsigned dynamic_smem_bytes() {
   return v;
 }
 
+// Block `rec` of the pattern table into bv[9].
+template <typename A>
+__device__ __forceinline__ void pt_block(const float *PT, int rec, A *bv) {
+  const float4 v0 = reinterpret_cast<const float4 *>(PT)[2 * rec];
+  const float4 v1 = reinterpret_cast<const float4 *>(PT)[2 * rec + 1];
+  bv[0] = (A)v0.x; bv[1] = (A)v0.y; bv[2] = (A)v0.z; bv[3] = (A)v0.w;
+  bv[4] = (A)v1.x; bv[5] = (A)v1.y; bv[6] = (A)v1.z; bv[7] = (A)v1.w;
+  bv[8] = (A)PT[8 * SP_PT_NREC + rec];
+}
+
 __device__ inline void stencil_ptable(int t, int nt, const double *Ke /*[2][576]*/, float *PT) {
-  for (int x = t; x < SP_PT_NREC * SP_PT_REC; x += nt) {
-    const int rec = x / SP_PT_REC, w = x % SP_PT_REC;
+  for (int x = t; x < SP_PT_NREC * 9; x += nt) {
+    const int rec = x < 8 * SP_PT_NREC ? x / 8 : x - 8 * SP_PT_NREC;
+    const int w = x < 8 * SP_PT_NREC ? x % 8 : 8;
     int m = 0;
     while (m < 26 && sp_pt_off(m + 1) <= rec) m++;
     const int p = rec - sp_pt_off(m);
     const int dx = m % 3 - 1, dy = (m / 3) % 3 - 1, dz = m / 9 - 1;
+    const int d = w / 3, cc = w % 3;
     double v = 0.0;
-    if (w < 9) {
-      const int d = w / 3, cc = w % 3;
-      int i = 0;
-      for (int c = 0; c < 8; c++) {
-        const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
-        const int bx = 1 - ox + dx, by = 1 - oy + dy, bz = 1 - oz + dz;
-        if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-        const int la = hex8_local(1 - ox, 1 - oy, 1 - oz), lb = hex8_local(bx, by, bz);
-        v += Ke[((p >> i) & 1) * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
-        i++;
-      }
+    int i = 0;
+    for (int c = 0; c < 8; c++) {
+      const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
+      const int bx = 1 - ox + dx, by = 1 - oy + dy, bz = 1 - oz + dz;
+      if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+      const int la = hex8_local(1 - ox, 1 - oy, 1 - oz), lb = hex8_local(bx, by, bz);
+      v += Ke[((p >> i) & 1) * SP_KE + (3 * la + d) * SP_NC + 3 * lb + cc];
+      i++;
     }
     PT[x] = (float)v;
   }
@@ -1051,7 +1062,7 @@ __device__ inline void spmm_stencil(int t, int nt, const MeshGeo &g, const T *KB
         for (int mm = 0; mm < 9; mm++) {
           const int dx = mm % 3 - 1, dy = mm / 3 - 1;
           A bv[9];
-          load_block<T, A>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
+          pt_block<A>(KB, sp_pt_index(mask, dx, dy, dz), bv);
           acc.fma_block(bv, x + nbk_base<K>(nbr_of(dx, dy, dz)), amask);
         }
       }
@@ -1183,7 +1194,7 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
 #pragma unroll
       for (int dx = -1; dx <= 1; dx++) {
         float bv[9];
-        load_block<float, float>(KB + sp_pt_index(mask, dx, dy, dz) * SP_PT_REC, bv);
+        pt_block<float>(KB, sp_pt_index(mask, dx, dy, dz), bv);
 #pragma unroll
         for (int p = 0; p < KP; p++) {
           if (!((amask >> (2 * p)) & 3u)) continue;
@@ -1309,7 +1320,7 @@ __device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const fl
         const int rec = s == 0 ? sp_pt_index(mask, 0, dy, dz)
                                : (s == 1 ? sp_pt_index(mR, -1, dy, dz) : sp_pt_index(mL, 1, dy, dz));
         float bv[9];
-        load_block<float, float>(KB + rec * SP_PT_REC, bv);
+        pt_block<float>(KB, rec, bv);
 #pragma unroll
         for (int p = 0; p < KP; p++) {
           if (!((amask >> (2 * p)) & 3u)) continue;
