@@ -1273,6 +1273,11 @@ __device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const fl
   const int esy = g.nex, esz = g.nex * g.ney;
   const size_t blk = (size_t)3 * g.nn_pad;
   const int ngr = (ni + 29) / 30;
+  // per-thread partial sums of x.y in FP32 (a few dozen terms), added to
+  // the caller's FP64 sums once: six fewer registers across the loop
+  float dotf[K];
+#pragma unroll
+  for (int q = 0; q < K; q++) dotf[q] = 0.f;
   for (int gi = warp; gi < ngr; gi += nwarps) {
     const int s0 = (rev ? ngr - 1 - gi : gi) * 30;
     const int id = s0 - 1 + lane;
@@ -1355,12 +1360,14 @@ __device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const fl
 #pragma unroll
         for (int d = 0; d < 3; d++) {
           const float yv = (q & 1) ? acc[0][d][q >> 1].y : acc[0][d][q >> 1].x;
-          dot[q] += (double)yv * (double)x[nbk_base<K>(a) + (d * K + q) * 32];
+          dotf[q] = fmaf(yv, x[nbk_base<K>(a) + (d * K + q) * 32], dotf[q]);
           y[q * blk + (size_t)d * g.nn_pad + a] = yv;
         }
       }
     }
   }
+#pragma unroll
+  for (int q = 0; q < K; q++) dot[q] += (double)dotf[q];
 }
 
 // b = -K u on interior dofs in stencil form (Dirichlet conditions): one
