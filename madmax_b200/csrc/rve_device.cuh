@@ -1255,10 +1255,15 @@ __device__ inline void spmm_stencil_xw(int t, int nt, const MeshGeo &g, const fl
 // warp trip (36 shuffles instead of 324 for the inputs), and are added only
 // where the neighbour is an interior node of the same row (the CG vectors
 // vanish on the Dirichlet boundary).  Same blocks and products as
-// spmm_stencil; the sums differ in order only.  The shared-memory pipe that
-// serves the shuffles, the pattern-table loads and the gathers' L1 hits is
-// what bounds this operator: this form needs 31% fewer of its wavefronts.
-// KB is the pattern table (stencil_ptable).
+// spmm_stencil; the sums differ in order only.  The L1 data pipe, which
+// serves the shuffles, the pattern-table loads and the gathers' L1 hits,
+// bounds this operator; the shuffles were a third of its wavefronts, and
+// the operator alone runs 22% faster in this form (n = 12..20).  The
+// per-thread x.y partial sums stay in FP32 until the end of the call (fewer
+// registers across the loop).  KB is the pattern table (stencil_ptable).
+// The gathers stay under the active-pair condition: in this kernel that
+// form compiles to the faster code (in a stand-alone harness it was the
+// reverse), so changes here are judged by the batched kernel's time.
 template <int K>
 __device__ inline void spmm_stencil_xo(int t, int nt, const MeshGeo &g, const float *KB,
                                        const uint8_t *__restrict__ etype,
